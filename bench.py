@@ -1,0 +1,516 @@
+#!/usr/bin/env python
+"""Benchmark: GTEPS of the six Polymer applications on one B200.
+
+One step runs the whole suite once on device-resident synthetic graphs:
+  graph A  symmetrised R-MAT scale 22, edge factor 16, int32 weights U{1..22}:
+           BFS from 16 seeded non-isolated sources, Connected Components,
+           BellmanFord from the first source
+  graph B  directed R-MAT scale 24, edge factor 16, float weights U(0,1]:
+           PageRank 20 iterations (FP32), SpMV 10 iterations, BP 10 iterations
+Edges counted (GTEPS numerator): BFS sum over sources of the out-degrees of
+the reached vertices; CC and BellmanFord m; PageRank/SpMV/BP m per iteration.
+value = counted edges / device time of the step (CUDA events on the graph
+streams), aggregated over ranks.  `e2e` repeats the suite through the public
+API from pinned host CSR arrays (graph upload + CSC build + results back).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS & %HBM peak per algo, 1 B200; batched/adjoint vs plain at FP64-tol"
+SEED_GRAPH, SEED_W, SEED_X, SEED_PRIOR, SEED_SRC = (0x5EED0001, 0x5EED0002, 0x5EED0003,
+                                                   0x5EED0004, 0x5EED0005)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale-a", type=int, default=22)
+    p.add_argument("--scale-b", type=int, default=24)
+    p.add_argument("--sources", type=int, default=16)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+class Suite:
+    """The two device-resident graphs and the per-step application calls."""
+
+    def __init__(self, pm, device, scale_a, scale_b, n_sources, rank):
+        self.pm = pm
+        t0 = time.time()
+        self.A = pm.Graph.rmat(scale_a, 16, seed=SEED_GRAPH, symmetric=True, device=device)
+        self.A.gen_weights_int(SEED_W, 22)
+        self.B = pm.Graph.rmat(scale_b, 16, seed=SEED_GRAPH, symmetric=False, device=device)
+        self.B.gen_weights_unit(SEED_W)
+        self.setup_s = time.time() - t0
+        offA, _ = self.A.csr()
+        self.sources = self._pick_sources(offA, n_sources, SEED_SRC + rank)
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        n = self.B.n
+        self.x0 = torch.from_numpy(self._uniform01(n, SEED_X)).to(self.dev)
+        self.prior = torch.from_numpy(self._uniform_open(2 * n, SEED_PRIOR)).to(self.dev).view(n, 2)
+        self.outA = torch.empty(self.A.n, dtype=torch.int32, device=self.dev)
+        self.outB = torch.empty(self.B.n, dtype=torch.float32, device=self.dev)
+        torch.cuda.synchronize(self.dev)
+
+    @staticmethod
+    def _hash(seed, c):
+        M = (1 << 64) - 1
+        z = (seed + (c + 1) * 0x9E3779B97F4A7C15) & M
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        return z ^ (z >> 31)
+
+    def _pick_sources(self, off, k, seed):
+        n = len(off) - 1
+        out = []
+        j = 0
+        while len(out) < k and j < 64 * n:
+            v = self._hash(seed, j) % n
+            j += 1
+            if off[v + 1] > off[v] and v not in out:
+                out.append(int(v))
+        return out
+
+    def _uniform01(self, n, seed):
+        return self.pm.uniform_f32(self.B, n, seed, open_interval=False).cpu().numpy()
+
+    def _uniform_open(self, n, seed):
+        return self.pm.uniform_f32(self.B, n, seed, open_interval=True).cpu().numpy()
+
+    def step(self, per):
+        """One pass of the suite; accumulates {algo: [ms, edges]} into per."""
+        pm, A, B = self.pm, self.A, self.B
+        total_ms, total_edges = 0.0, 0
+
+        def rec(name, ms, edges):
+            nonlocal total_ms, total_edges
+            e = per.setdefault(name, [0.0, 0])
+            e[0] += ms
+            e[1] += edges
+            total_ms += ms
+            total_edges += edges
+
+        for s in self.sources:
+            A.timer_begin()
+            _, _, st = pm.BFS(s, A, device_out=self.outA, stats=True)
+            rec("bfs", A.timer_end(), st["edges_visited"])
+        A.timer_begin()
+        pm.Components(A, device_out=self.outA)
+        rec("cc", A.timer_end(), A.m)
+        A.timer_begin()
+        pm.BellmanFord(A, self.sources[0], device_out=self.outA)
+        rec("bellman_ford", A.timer_end(), A.m)
+        B.timer_begin()
+        pm.PageRank(B, 20, dtype=np.float32, device_out=self.outB)
+        rec("pagerank", B.timer_end(), B.m * 20)
+        B.timer_begin()
+        pm.SPMV(B, self.x0, 10)
+        rec("spmv", B.timer_end(), B.m * 10)
+        B.timer_begin()
+        pm.BeliefPropagation(B, self.prior, 10)
+        rec("bp", B.timer_end(), B.m * 10)
+        return total_ms, total_edges
+
+
+def e2e_run(pm, suite, steps):
+    """Suite through the public API from pinned host CSR arrays, per step:
+    upload + build both graphs, set weights, run, read every result back."""
+    A, B = suite.A, suite.B
+    hA = {k: pm.PinnedArray(c, t) for k, (c, t) in
+          {"off": (A.n + 1, np.int32), "idx": (A.m, np.int32), "w": (A.m, np.int32)}.items()}
+    hB = {k: pm.PinnedArray(c, t) for k, (c, t) in
+          {"off": (B.n + 1, np.int32), "idx": (B.m, np.int32), "w": (B.m, np.float32),
+           "x0": (B.n, np.float32), "prior": (2 * B.n, np.float32)}.items()}
+    oA, iA = A.csr()
+    hA["off"].array[:] = oA
+    hA["idx"].array[:] = iA
+    hA["w"].array[:] = A.weights_i32()
+    oB, iB = B.csr()
+    hB["off"].array[:] = oB
+    hB["idx"].array[:] = iB
+    hB["w"].array[:] = B.weights_f32()
+    hB["x0"].array[:] = suite.x0.cpu().numpy()
+    hB["prior"].array[:] = suite.prior.cpu().numpy().reshape(-1)
+    h2d = sum(a.array.nbytes for a in hA.values()) + sum(a.array.nbytes for a in hB.values())
+    d2h = 0
+    times, edges = [], 0
+    for _ in range(steps):
+        suite.torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e = 0
+        d2h = 0
+        with pm.Graph.from_csr(hA["off"].array, hA["idx"].array, symmetric=True) as gA:
+            gA.set_weights(hA["w"].array)
+            for s in suite.sources:
+                p, d, st = pm.BFS(s, gA, stats=True)
+                e += st["edges_visited"]
+                d2h += p.nbytes + d.nbytes
+            lab = pm.Components(gA)
+            dist = pm.BellmanFord(gA, suite.sources[0])
+            e += 2 * gA.m
+            d2h += lab.nbytes + dist.nbytes
+        with pm.Graph.from_csr(hB["off"].array, hB["idx"].array) as gB:
+            gB.set_weights(hB["w"].array)
+            r = pm.PageRank(gB, 20, dtype=np.float32)
+            y = pm.SPMV(gB, hB["x0"].array, 10)
+            lp = pm.BeliefPropagation(gB, hB["prior"].array.reshape(-1, 2), 10)
+            e += gB.m * 40
+            d2h += r.nbytes + y.nbytes + lp.nbytes
+        times.append(time.perf_counter() - t0)
+        edges = e
+    for a in list(hA.values()) + list(hB.values()):
+        a.free()
+    t = statistics.median(times)
+    return {"value": round(edges / t / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t, 4),
+            "timing": "host clock around synchronous API calls, median of %d steps" % steps}
+
+
+def ncu_traffic():
+    """DRAM bytes per PageRank pass from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "pagerank_pull_scale24.md")
+    try:
+        for ln in open(path):
+            if ln.strip().startswith("traffic_bytes_per_pass:"):
+                return float(ln.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference binaries (oracle/_ref) or the oracle port.
+# ---------------------------------------------------------------------------
+class CpuSample:
+    """Bounded sample of the suite for the CPU: the same applications and
+    edge-count rules on smaller graphs (scale given), files written once."""
+
+    def __init__(self, scale, n_sources=2, wscale=None):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pm_oracle as O
+        self.O = O
+        self.scale = scale
+        self.wscale = wscale or scale
+        self.d = O.tempdir()
+        self.gd = O.rmat_graph(scale, 16)
+        self.gs = O.rmat_graph(scale, 16, symmetric=True)
+        self.gdw = self.gd if self.wscale == scale else O.rmat_graph(self.wscale, 16)
+        self.gsw = self.gs if self.wscale == scale else O.rmat_graph(self.wscale, 16, symmetric=True)
+        self.kind = "reference" if O.ref_available() else "port"
+        self.sources = [int(s) for s in O.pick_sources(self.gs, n_sources)]
+        self.bf_src = int(O.pick_sources(self.gsw, 1)[0])
+        deg = np.diff(self.gs.off)
+        self.bfs_edges = []
+        for s in self.sources:
+            depth, _ = O.bfs(self.gs, s)
+            self.bfs_edges.append(int(deg[depth >= 0].sum()))
+        if self.kind == "reference":
+            self.bd = O.write_binary(self.gd, os.path.join(self.d, "dir"))
+            self.bs = O.write_binary(self.gs, os.path.join(self.d, "sym"))
+            self.tw_sym = os.path.join(self.d, "symw.txt")
+            O.write_text(self.gsw, self.tw_sym, O.weights_int(self.gsw))
+            # the reference SpMV reads int weights (numa-SPMV.C:72); same graph, U{1..22}
+            self.tw_dir = os.path.join(self.d, "dirw.txt")
+            O.write_text(self.gdw, self.tw_dir, O.weights_int(self.gdw))
+        else:
+            self.w_sym = O.weights_int(self.gsw)
+            self.w_dir = O.weights_unit(self.gdw).astype(np.float64)
+            self.x0 = O.uniform01(self.gdw.n).astype(np.float64)
+            self.prior = O.uniform_open(2 * self.gd.n).reshape(-1, 2).astype(np.float64)
+
+    def describe(self):
+        return ("R-MAT scale %d (PageRank 20 it, BP 10 it; BFS x%d, CC on the symmetrised graph), "
+                "scale %d weighted (SpMV 10 it, BellmanFord x1)" % (self.scale, len(self.sources),
+                                                                    self.wscale))
+
+    def step(self, threads):
+        """Runs the sample once; returns (seconds, edges, per-algo dict)."""
+        O = self.O
+        per = {}
+        if self.kind == "reference":
+            _, t = O.ref_pagerank(self.bd, 20, threads=threads, result=False)
+            per["pagerank"] = (t, self.gd.m * 20)
+            t = O.ref_bp(self.bd, 10, threads=threads)
+            per["bp"] = (t, self.gd.m * 10)
+            _, t = O.ref_spmv(self.tw_dir, 10, threads=threads, result=False)
+            per["spmv"] = (t, self.gdw.m * 10)
+            tb = 0.0
+            for s in self.sources:
+                _, _, t = O.ref_bfs(self.bs, s, threads=threads, parents=False)
+                tb += t
+            per["bfs"] = (tb, sum(self.bfs_edges))
+            _, t = O.ref_components(self.bs, threads=threads, result=False)
+            per["cc"] = (t, self.gs.m)
+            _, t = O.ref_bellman_ford(self.tw_sym, self.bf_src, threads=threads)
+            per["bellman_ford"] = (t, self.gsw.m)
+        else:
+            def timed(fn):
+                t0 = time.perf_counter()
+                fn()
+                return time.perf_counter() - t0
+            per["pagerank"] = (timed(lambda: O.pagerank(self.gd, 20)), self.gd.m * 20)
+            per["bp"] = (timed(lambda: O.bp(self.gd, self.prior, 10)), self.gd.m * 10)
+            per["spmv"] = (timed(lambda: O.spmv(self.gdw, self.w_dir, self.x0, 10)), self.gdw.m * 10)
+            per["bfs"] = (sum(timed(lambda s=s: O.bfs(self.gs, s)) for s in self.sources),
+                          sum(self.bfs_edges))
+            per["cc"] = (timed(lambda: O.cc(self.gs)), self.gs.m)
+            per["bellman_ford"] = (timed(lambda: O.bellman_ford(self.gsw, self.w_sym, self.bf_src)),
+                                   self.gsw.m)
+        secs = sum(v[0] for v in per.values())
+        edges = sum(v[1] for v in per.values())
+        return secs, edges, per
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline():
+    threads = cpu_threads()
+    s = CpuSample(18, n_sources=2, wscale=17)
+    secs, edges, per = s.step(threads if s.kind == "reference" else 1)
+    return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS",
+            "cores": threads if s.kind == "reference" else 1, "kind": s.kind,
+            "sample": s.describe() + "; one pass, each application's own timer",
+            "per_algo": {k: round(v[1] / v[0] / 1e9, 5) for k, v in per.items()}}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    threads = cpu_threads()
+    s = CpuSample(18, n_sources=2, wscale=17)
+    for _ in range(args.warmup):
+        s.step(threads)
+    tot_s, tot_e = 0.0, 0
+    per = {}
+    for _ in range(args.steps):
+        secs, edges, p = s.step(threads)
+        tot_s += secs
+        tot_e += edges
+        for k, v in p.items():
+            a = per.setdefault(k, [0.0, 0])
+            a[0] += v[0]
+            a[1] += v[1]
+    value = tot_e / tot_s / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GTEPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * tot_s / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/i32", "data": "synthetic",
+        "config": {"workload": "six-application suite, CPU sample: " + s.describe(),
+                   "threads": threads, "kind": s.kind},
+        "per_algo": {k: {"gteps": round(v[1] / v[0] / 1e9, 5), "ms": round(1000 * v[0] / args.steps, 3)}
+                     for k, v in per.items()},
+        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": threads, "kind": s.kind,
+                         "sample": s.describe()},
+        "e2e": {"value": round(value, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import polymer_b200 as pm
+    suite = Suite(pm, local, args.scale_a, args.scale_b, args.sources, rank)
+    per = {}
+    for _ in range(args.warmup):
+        suite.step({})
+    # roofline source: per-pass device time of the PageRank pull-reduce
+    suite.B.profile(True)
+    suite.B.profile_read("pagerank", reset=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = pm.kernel_launches()
+    tot_ms, tot_edges = 0.0, 0
+    for _ in range(args.steps):
+        ms, e = suite.step(per)
+        tot_ms += ms
+        tot_edges += e
+    torch.cuda.synchronize()
+    launches = pm.kernel_launches() - launches0
+    clk = clocks.stop()
+    pr_ms, pr_passes = suite.B.profile_read("pagerank", reset=True)
+    suite.B.profile(False)
+    ms_step = tot_ms / args.steps
+    if dist:
+        t = torch.tensor([ms_step, float(tot_edges)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_step, tot_edges_all = float(mx[0]), float(sm[1])
+    else:
+        tot_edges_all = float(tot_edges)
+    value = tot_edges_all / args.steps / (ms_step / 1e3) / 1e9
+    hbm, peak_kind = peaks()
+    nB, mB = suite.B.n, suite.B.m
+    pass_bytes = 8 * mB + 32 * nB
+    pass_ms = pr_ms / max(pr_passes, 1)
+    achieved = pass_bytes / (pass_ms / 1e3) / 1e9 if pr_passes else None
+    per_algo = {}
+    algo_bytes = {  # algorithmic bytes per counted edge-unit, see DESIGN.md
+        "pagerank": lambda: (8 * mB + 32 * nB) * 20, "spmv": lambda: (12 * mB + 12 * nB) * 10,
+        "bp": lambda: (4 * mB + 40 * nB) * 10,
+    }
+    for k, (ms, e) in per.items():
+        d = {"gteps": round(e / (ms / 1e3) / 1e9, 3), "ms_per_step": round(ms / args.steps, 3)}
+        if k in algo_bytes:
+            gbs = algo_bytes[k]() * args.steps / (ms / 1e3) / 1e9
+            d["hbm_gbs"] = round(gbs, 1)
+            d["hbm_frac"] = round(gbs / hbm, 4)
+        per_algo[k] = d
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32",
+        "data": "synthetic",
+        "config": {
+            "workload": "six-application suite: BFS x%d + CC + BellmanFord on symmetrised R-MAT "
+                        "scale %d ef16 (n=%d, m=%d); PageRank 20 it + SpMV 10 it + BP 10 it on "
+                        "directed R-MAT scale %d ef16 (n=%d, m=%d)"
+                        % (len(suite.sources), args.scale_a, suite.A.n, suite.A.m, args.scale_b,
+                           nB, mB),
+            "graphs": {"A": {"scale": args.scale_a, "n": suite.A.n, "m": suite.A.m},
+                       "B": {"scale": args.scale_b, "n": nB, "m": mB}},
+            "l2": "inputs larger than L2 (126 MB): graph A ids %d MB, graph B ids %d MB"
+                  % (suite.A.m * 4 >> 20, mB * 4 >> 20),
+            "parallelism": "replicas x%d" % world,
+        },
+        "per_algo": per_algo,
+        "roofline": {
+            "kernel": "PageRank pull-reduce pass (k_heavy_reduce + k_pull_reduce<PR_F<float>>)",
+            "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+            "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4) if achieved else None,
+            "traffic": ncu_traffic(), "algorithmic_bytes_per_pass": pass_bytes,
+            "pass_ms": round(pass_ms, 4), "passes": pr_passes,
+        },
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as exc:  # keep the GPU line even if the CPU sample fails
+            line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    if not args.no_e2e:
+        line["e2e"] = e2e_run(pm, suite, args.e2e_steps)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

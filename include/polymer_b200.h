@@ -1,0 +1,199 @@
+/*
+ * polymer_b200.h -- C ABI of the B200 edgeMap/vertexMap engine.
+ *
+ * Polymer has no FFI of its own: its applications are C++ programs whose
+ * entry functions (PageRank(), BFS(), Components(), BF_main(), SPMV_main(),
+ * BeliefPropagation()) take a graph built by readGraph() and run the hot
+ * loops on CPU threads.  Each entry point below replaces one of those
+ * functions (cited as file:line of the reference), with plain pointers and
+ * sizes, so that a C, C++, Go (cgo), Java (JNI) or Python (ctypes) host can
+ * call it.  Every function returns a pm_status and never aborts; the text
+ * of the last error on the calling thread is pm_last_error().
+ *
+ * Memory: arrays passed with PM_MEM_HOST are ordinary host memory (pinned
+ * or pageable); PM_MEM_DEVICE arrays are device pointers on the graph's
+ * device.  Calls are synchronous: on return every output has been written.
+ * A graph handle owns its device copy of the graph (CSR + CSC, int32 ids and
+ * offsets), its frontier workspaces and a CUDA stream; distinct handles may
+ * be used from distinct host threads.
+ */
+#ifndef POLYMER_B200_H
+#define POLYMER_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PM_API __attribute__((visibility("default")))
+#else
+#define PM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pm_status {
+  PM_OK = 0,
+  PM_ERR_INVALID_ARG = 1, /* bad size, id out of range, null pointer      */
+  PM_ERR_OOM = 2,         /* device or pinned allocation failed            */
+  PM_ERR_CUDA = 3,        /* a CUDA runtime call failed                   */
+  PM_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up            */
+  PM_ERR_BAD_GRAPH = 5,   /* offsets not monotone, edge id out of range   */
+  PM_ERR_NOT_SUPPORTED = 6,
+  PM_ERR_NO_DEVICE = 7
+} pm_status;
+
+typedef struct pm_graph pm_graph;
+
+/* memory-space flags for array arguments */
+#define PM_MEM_HOST 0u
+#define PM_MEM_DEVICE 1u
+
+/* pm_graph_create flags */
+#define PM_GRAPH_SYMMETRIC 2u       /* CSR already holds both directions (the
+                                       reference's "-s" flag): CSC aliases CSR */
+#define PM_GRAPH_SKIP_SELF_LOOPS 4u /* drop u->u edges while loading, as
+                                       readGraphSkipRing does (IO-numa.h:192) */
+#define PM_GRAPH_KEEP_EDGE_IDS 8u   /* keep the CSC->CSR edge-id map resident */
+
+/* value types */
+#define PM_F32 0
+#define PM_F64 1
+
+/* Build a device graph from a CSR (PBBS AdjacencyGraph layout: offsets of
+ * n+1 entries -- append m to the n offsets a PBBS file holds -- and m
+ * destination ids).  Replaces readGraph()/readGraphSkipRing()
+ * (IO-numa.h:739-750), which build graph<vertex> with in-edges by sorting
+ * (dst, src) pairs (IO-numa.h:145-180); here the CSC is built on the device.
+ * mem: PM_MEM_HOST or PM_MEM_DEVICE for offsets/edges. */
+PM_API pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t n, int64_t m,
+                          uint32_t flags, uint32_t mem, int device, pm_graph **out);
+
+/* Build the seeded synthetic R-MAT graph (a,b,c,d = .57,.19,.19,.05;
+ * n = 2^scale, n*edge_factor draws, self loops and duplicates removed,
+ * sorted by source) directly on the device.  The same generator, evaluated
+ * on the CPU, produces the same edge set.  PM_GRAPH_SYMMETRIC symmetrises
+ * (union of both directions).  The reference ships no generator. */
+PM_API pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32_t flags,
+                               int device, pm_graph **out);
+
+PM_API pm_status pm_graph_destroy(pm_graph *g);
+
+/* n, m (directed stored edges) and max out-degree. */
+PM_API pm_status pm_graph_info(const pm_graph *g, int64_t *n, int64_t *m, int64_t *max_out_degree);
+
+/* Copy the CSR back (offsets n+1, edges m). */
+PM_API pm_status pm_graph_get_csr(pm_graph *g, int32_t *offsets, int32_t *edges, uint32_t mem);
+
+/* Edge weights in CSR order, as the weighted readers attach them
+ * (readWghGraph, IO-numa.h:318-402 / IO.h; weights at neighbors[2j+1],
+ * graph.h:89-113).  int32 for BellmanFord, float for SpMV. */
+PM_API pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem);
+PM_API pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem);
+/* Synthetic weights on the device: int32 uniform in [1, wmax] with
+ * w(u,v) == w(v,u); float uniform in (0, 1]. Same rules as the oracle. */
+PM_API pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax);
+PM_API pm_status pm_graph_gen_weights_f32(pm_graph *g, uint64_t seed);
+/* Read the weights back in CSR order. */
+PM_API pm_status pm_graph_get_weights_f32(pm_graph *g, float *w, uint32_t mem);
+PM_API pm_status pm_graph_get_weights_i32(pm_graph *g, int32_t *w, uint32_t mem);
+
+/* Seeded uniform vectors on the device ([0,1) or (0,1)), for synthetic
+ * SpMV / BP inputs. out is a device array of count floats. */
+PM_API pm_status pm_fill_uniform_f32(pm_graph *g, uint64_t seed, int open_interval, float *out,
+                              int64_t count);
+
+typedef struct pm_traversal_stats {
+  int32_t rounds;         /* edgeMap calls until the frontier emptied       */
+  int32_t dense_rounds;   /* of which took the dense (pull) direction       */
+  int64_t edges_visited;  /* sum over rounds of the out-degree of the frontier
+                             (the edges a push traversal scans)             */
+  int64_t reached;        /* vertices with a finite result                  */
+} pm_traversal_stats;
+
+/* Breadth-first search from src.  Replaces BFS(start, GA) (numa-BFS.C:476)
+ * with BFS_F (numa-BFS.C:59-79): parents[v] = some in-neighbour one level
+ * up (parents[src] = src, -1 when unreached); depth[v] = level (or -1).
+ * Either output may be NULL.  threshold: direction switch, dense (pull)
+ * when |F| + outdeg(F) >= threshold; < 0 selects m/20; 0 forces dense
+ * every level as the reference's BFS does (numa-BFS.C:268). */
+PM_API pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
+                 int64_t threshold, pm_traversal_stats *stats);
+
+/* Connected components by min-label propagation.  Replaces Components(GA)
+ * (numa-Components.C:402) with CC_F / CC_Vertex_F (55-119): labels start at
+ * the vertex id, every round lowers labels along the out-edges of the
+ * frontier (vertices whose label fell).  threshold < 0 selects m/8
+ * (numa-Components.C:226). labels: n int32. */
+PM_API pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t threshold,
+                        pm_traversal_stats *stats);
+
+/* Single-source shortest paths by Bellman-Ford over int32 weights
+ * (pm_graph_set_weights_i32).  Replaces BF_main(WG, start)
+ * (numa-BellmanFord.C:400) with BF_F (61-85): dist starts at 1073741823
+ * (INT_MAX/2, 283), dist[src] = 0, a vertex joins the next frontier when
+ * its distance falls in the round.  threshold < 0 selects m/20 (182). */
+PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem,
+                          int64_t threshold, pm_traversal_stats *stats);
+
+/* PageRank with Polymer's frontier semantics.  Replaces PageRank(GA,
+ * maxIter) (numa-PageRank.C:548) with PR_F / PR_Vertex_F / PR_Vertex_Reset
+ * (64-148) and the loop at 273-335: p = 1/n on all vertices, each iteration
+ * pushes p[s]/outdeg(s) from the frontier, damps the frontier's entries,
+ * zeroes them in the old vector, swaps, and the next frontier is the set of
+ * vertices that received a push.  The graph must have no self loops.
+ * dtype PM_F32 (FP32 storage and sums) or PM_F64; ranks: n values of dtype.
+ * resid (optional, iters doubles): sum |p_{t+1} - p_t| per iteration, FP64. */
+PM_API pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *ranks,
+                      uint32_t mem, double *resid);
+
+/* Weighted SpMV power iteration over the float weights.  Replaces
+ * SPMV_main(WG, maxIter) (numa-SPMV.C:335) with SPMV_F (56-97): every
+ * iteration y[d] = sum_{s->d} w(s,d) x[s] over all vertices, then x = y.
+ * x0: n floats (the reference starts from 1/n, numa-SPMV.C:271). y: n
+ * floats. norm1 (optional, iters doubles): FP64 L1 norm of each y. */
+PM_API pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem,
+                  double *norm1);
+
+/* Two-state belief propagation.  Replaces BeliefPropagation(G, maxIter)
+ * (numa-BP.C:528) with BP_F / BP_Vertex_Reset (89-140) and
+ * edgeMapDenseBPNoRep (179-230): for every out-edge s->d of the frontier,
+ * belief[i] = sum_j prior_d[j] psi[i][j] prod_d[j], prod'_d[i] *= belief[i];
+ * prod' resets to 1 on the frontier; the next frontier is every vertex that
+ * received a message.  Products start at 1 and are carried as natural logs
+ * (log_prod, n x 2 floats) so that vertices with thousands of in-edges do
+ * not underflow.  prior: n x 2 floats; psi: 4 floats [i][j], shared by all
+ * edges. */
+PM_API pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
+                uint32_t mem);
+
+/* Device timing on the graph's stream (CUDA events): begin, then end
+ * returns the elapsed milliseconds. */
+PM_API pm_status pm_timer_begin(pm_graph *g);
+PM_API pm_status pm_timer_end(pm_graph *g, float *ms);
+
+/* Per-pass device profile.  When enabled, every edgeMap pass of an
+ * application (one PageRank / SpMV / BP iteration, one BFS / CC /
+ * BellmanFord round) is bracketed by CUDA events on the graph's stream.
+ * pm_profile_read sums the passes recorded under tag ("pagerank",
+ * "spmv", "bp", "bfs", "cc", "bellman_ford"): total milliseconds and count;
+ * reset clears the records.  No counterpart in the reference, whose only
+ * timers are gettimeofday() around whole runs (gettime.h:30-113). */
+PM_API pm_status pm_profile_enable(pm_graph *g, int enable);
+PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_t *passes,
+                                 int reset);
+
+/* Pinned (page-locked) host memory for fast host<->device staging. */
+PM_API pm_status pm_host_alloc(uint64_t bytes, void **out);
+PM_API pm_status pm_host_free(void *p);
+
+/* Number of kernels this library launched since the last reset. */
+PM_API int64_t pm_kernel_launches(int reset);
+
+PM_API const char *pm_last_error(void);
+PM_API const char *pm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POLYMER_B200_H */

@@ -1,0 +1,369 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE, not product).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.  It loads ``_build/libpm_oracle.so`` (the C
+restatement in ``pm_oracle.c``) and drives the reference binaries in ``_ref/``
+(compiled from the original Polymer sources by ``oracle/Makefile``).
+
+Graph convention: CSR ``off`` (int32, n+1) and ``idx`` (int32, m), edges
+sorted by (source, destination), no self loops, no duplicates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libpm_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+BF_INF = 1073741823  # INT_MAX / 2, numa-BellmanFord.C:283
+SEED_GRAPH = 0x5EED0001
+SEED_WEIGHT = 0x5EED0002
+SEED_X = 0x5EED0003
+SEED_PRIOR = 0x5EED0004
+SEED_SOURCES = 0x5EED0005
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the C restatement (and, when the reference sources are
+    present, the reference binaries) with make."""
+    targets = ["oracle"]
+    if os.path.isdir("/root/reference"):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        i64, u64, i32 = C.c_int64, C.c_uint64, C.c_int32
+        sig = {
+            "pmo_hash": (u64, [u64, u64]),
+            "pmo_rmat_edge": (u64, [C.c_int, u64, u64]),
+            "pmo_keys_to_csr": (i64, [u64p, i64, i64, C.c_int, i32p, i32p]),
+            "pmo_rmat_graph": (i64, [C.c_int, C.c_int, u64, C.c_int, i32p, i32p]),
+            "pmo_fill_weights_int": (None, [i64, i32p, i32p, u64, i32, i32p]),
+            "pmo_fill_weights_unit": (None, [i64, i32p, i32p, u64, f32p]),
+            "pmo_fill_uniform01": (None, [u64, i64, f32p]),
+            "pmo_fill_uniform_open": (None, [u64, i64, f32p]),
+            "pmo_pick_sources": (C.c_int, [i64, i32p, u64, C.c_int, i32p]),
+            "pmo_transpose": (None, [i64, i32p, i32p, i32p, i32p, C.c_void_p]),
+            "pmo_pagerank": (None, [i64, i32p, i32p, C.c_int, C.c_double, f64p, C.c_void_p]),
+            "pmo_spmv": (None, [i64, i32p, i32p, f64p, f64p, C.c_int, f64p]),
+            "pmo_bfs": (i64, [i64, i32p, i32p, i32, i32p, C.c_void_p]),
+            "pmo_cc": (C.c_int, [i64, i32p, i32p, i32p]),
+            "pmo_bellman_ford": (C.c_int, [i64, i32p, i32p, i32p, i32, i32p]),
+            "pmo_dijkstra": (None, [i64, i32p, i32p, i32p, i32, i32p]),
+            "pmo_bp": (None, [i64, i32p, i32p, f64p, C.c_void_p, f64p, C.c_int, f64p]),
+            "pmo_write_adj_text": (C.c_int, [C.c_char_p, i64, i32p, i32p, C.c_void_p]),
+            "pmo_write_adj_binary": (C.c_int, [C.c_char_p, i64, i32p, i32p]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class Graph:
+    n: int
+    off: np.ndarray  # int32 [n+1]
+    idx: np.ndarray  # int32 [m]
+
+    @property
+    def m(self) -> int:
+        return int(self.off[-1])
+
+    def transpose(self):
+        toff = np.empty(self.n + 1, np.int32)
+        tidx = np.empty(max(self.m, 1), np.int32)
+        eid = np.empty(max(self.m, 1), np.int32)
+        lib().pmo_transpose(self.n, self.off, self.idx, toff, tidx, _ptr(eid))
+        return toff, tidx[: self.m], eid[: self.m]
+
+    def out_degree(self) -> np.ndarray:
+        return np.diff(self.off).astype(np.int64)
+
+
+def rmat_graph(scale: int, ef: int, seed: int = SEED_GRAPH, symmetric: bool = False) -> Graph:
+    """Seeded R-MAT (a,b,c,d) = (.57,.19,.19,.05), self loops and duplicates
+    removed, sorted by source: the synthetic input of every workload."""
+    n = 1 << scale
+    cap = n * ef * (2 if symmetric else 1)
+    off = np.empty(n + 1, np.int32)
+    idx = np.empty(max(cap, 1), np.int32)
+    m = lib().pmo_rmat_graph(scale, ef, seed, int(symmetric), off, idx)
+    return Graph(n, off, idx[:m].copy())
+
+
+def graph_from_edges(n: int, src, dst, symmetric: bool = False) -> Graph:
+    """CSR from an explicit edge list (dedup, self loops dropped)."""
+    src = np.asarray(src, np.uint64)
+    dst = np.asarray(dst, np.uint64)
+    keys = np.empty(max(2 * len(src), 1), np.uint64)
+    keys[: len(src)] = (src << np.uint64(32)) | dst
+    off = np.empty(n + 1, np.int32)
+    idx = np.empty(max(2 * len(src), 1), np.int32)
+    m = lib().pmo_keys_to_csr(keys, len(src), n, int(symmetric), off, idx)
+    return Graph(n, off, idx[:m].copy())
+
+
+def weights_int(g: Graph, seed: int = SEED_WEIGHT, wmax: int = 22) -> np.ndarray:
+    w = np.empty(max(g.m, 1), np.int32)
+    lib().pmo_fill_weights_int(g.n, g.off, g.idx if g.m else np.zeros(1, np.int32), seed, wmax, w)
+    return w[: g.m]
+
+
+def weights_unit(g: Graph, seed: int = SEED_WEIGHT) -> np.ndarray:
+    w = np.empty(max(g.m, 1), np.float32)
+    lib().pmo_fill_weights_unit(g.n, g.off, g.idx if g.m else np.zeros(1, np.int32), seed, w)
+    return w[: g.m]
+
+
+def uniform01(count: int, seed: int = SEED_X) -> np.ndarray:
+    x = np.empty(max(count, 1), np.float32)
+    lib().pmo_fill_uniform01(seed, count, x)
+    return x[:count]
+
+
+def uniform_open(count: int, seed: int = SEED_PRIOR) -> np.ndarray:
+    x = np.empty(max(count, 1), np.float32)
+    lib().pmo_fill_uniform_open(seed, count, x)
+    return x[:count]
+
+
+def pick_sources(g: Graph, k: int, seed: int = SEED_SOURCES) -> np.ndarray:
+    out = np.zeros(k, np.int32)
+    got = lib().pmo_pick_sources(g.n, g.off, seed, k, out)
+    return out[:got]
+
+
+def _idx(g: Graph):
+    return g.idx if g.m else np.zeros(1, np.int32)
+
+
+def pagerank(g: Graph, iters: int, damping: float = 0.85, with_resid: bool = False):
+    out = np.empty(g.n, np.float64)
+    resid = np.zeros(max(iters, 1), np.float64)
+    lib().pmo_pagerank(g.n, g.off, _idx(g), iters, damping, out, _ptr(resid))
+    return (out, resid[:iters]) if with_resid else out
+
+
+def spmv(g: Graph, w, x0, iters: int) -> np.ndarray:
+    out = np.empty(g.n, np.float64)
+    w64 = np.ascontiguousarray(w, np.float64) if g.m else np.zeros(1, np.float64)
+    lib().pmo_spmv(g.n, g.off, _idx(g), w64, np.ascontiguousarray(x0, np.float64), iters, out)
+    return out
+
+
+def bfs(g: Graph, src: int):
+    depth = np.empty(g.n, np.int32)
+    parents = np.empty(g.n, np.int32)
+    lib().pmo_bfs(g.n, g.off, _idx(g), src, depth, _ptr(parents))
+    return depth, parents
+
+
+def cc(g: Graph) -> np.ndarray:
+    labels = np.empty(g.n, np.int32)
+    lib().pmo_cc(g.n, g.off, _idx(g), labels)
+    return labels
+
+
+def bellman_ford(g: Graph, w, src: int) -> np.ndarray:
+    dist = np.empty(g.n, np.int32)
+    w32 = np.ascontiguousarray(w, np.int32) if g.m else np.zeros(1, np.int32)
+    lib().pmo_bellman_ford(g.n, g.off, _idx(g), w32, src, dist)
+    return dist
+
+
+def dijkstra(g: Graph, w, src: int) -> np.ndarray:
+    dist = np.empty(g.n, np.int32)
+    w32 = np.ascontiguousarray(w, np.int32) if g.m else np.zeros(1, np.int32)
+    lib().pmo_dijkstra(g.n, g.off, _idx(g), w32, src, dist)
+    return dist
+
+
+def bp(g: Graph, prior, iters: int, psi_uniform=None, psi_edge=None) -> np.ndarray:
+    """Log-products (n x 2) of the 2-state BP restatement."""
+    out = np.empty(2 * g.n, np.float64)
+    pu = np.ascontiguousarray(
+        psi_uniform if psi_uniform is not None else [[0.9, 0.1], [0.1, 0.9]], np.float64
+    ).reshape(4)
+    pe = None if psi_edge is None else np.ascontiguousarray(psi_edge, np.float64).reshape(-1)
+    lib().pmo_bp(g.n, g.off, _idx(g), np.ascontiguousarray(prior, np.float64).reshape(-1),
+                 _ptr(pe), pu, iters, out)
+    return out.reshape(g.n, 2)
+
+
+def bfs_depths_from_parents(parents: np.ndarray, src: int) -> np.ndarray:
+    """Depth of every vertex by walking the parent array (-1: unreached).
+    Raises ValueError on a cycle or a parent chain that misses src."""
+    n = len(parents)
+    depth = np.full(n, -2, np.int64)
+    depth[parents < 0] = -1
+    depth[src] = 0
+    for v in range(n):
+        if depth[v] != -2:
+            continue
+        chain = []
+        u = v
+        while depth[u] == -2:
+            chain.append(u)
+            u = int(parents[u])
+            if u < 0 or len(chain) > n:
+                raise ValueError("broken parent chain at %d" % v)
+        base = depth[u]
+        if base < 0:
+            raise ValueError("parent chain of %d reaches an unreached vertex" % v)
+        for k, x in enumerate(reversed(chain)):
+            depth[x] = base + 1 + k
+    return depth.astype(np.int32)
+
+
+# ------------------------------------------------------------------------
+# Reference binaries (compiled by oracle/Makefile into _ref/).
+# ------------------------------------------------------------------------
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "numa-PageRank"))
+
+
+def write_binary(g: Graph, base: str) -> str:
+    """Write <base>.config/.adj/.idx and return the base name to pass to the
+    reference.  The reference's binary loaders copy "<base>.config" (len+8
+    bytes with the NUL) into char[len+7] and "<base>.adj"/".idx" (len+5) into
+    char[len+4] stack arrays (IO-numa.h:409-417); the extra byte lands in the
+    16-byte alignment padding of those arrays unless len+7 or len+4 is a
+    multiple of 16, where the program can abort.  Such lengths get a suffix."""
+    while len(base) % 16 in (9, 12):
+        base = base + "_"
+    if lib().pmo_write_adj_binary(base.encode(), g.n, g.off, _idx(g)) != 0:
+        raise OSError("cannot write %s" % base)
+    return base
+
+
+def write_text(g: Graph, path: str, w=None) -> None:
+    wp = None if w is None else np.ascontiguousarray(w, np.int32)
+    if lib().pmo_write_adj_text(path.encode(), g.n, g.off, _idx(g), _ptr(wp)) != 0:
+        raise OSError("cannot write %s" % path)
+
+
+_TIME_RE = re.compile(r"^(PageRank|BFS|Components|BellmanFord|SPMV|BeliefPropagation)\s*:\s*([0-9.eE+-]+)", re.M)
+
+
+def _run(args, threads: int | None, timeout: float):
+    env = dict(os.environ)
+    if threads:
+        env["PM_REF_THREADS"] = str(threads)
+    p = subprocess.run(args, capture_output=True, text=True, env=env, timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError("reference %s failed (%d): %s" % (args[0], p.returncode, p.stderr[-400:]))
+    t = _TIME_RE.findall(p.stdout)
+    return p.stdout, (float(t[-1][1]) if t else float("nan"))
+
+
+def ref_pagerank(path: str, iters: int, binary: bool = True, threads=None, result=True, timeout=600):
+    """numa-PageRank <g> <iters> -1 [-result] [-s] [-b]; returns (ranks|None, seconds)."""
+    args = [os.path.join(REF_DIR, "numa-PageRank"), path, str(iters), "-1",
+            "-result" if result else "-noresult", "-a", "-b" if binary else "-t"]
+    out, t = _run(args, threads, timeout)
+    if not result:
+        return None, t
+    vals = re.findall(r"^(\d+)\t([0-9.eE+-]+)$", out, re.M)
+    r = np.zeros(len(vals), np.float64)
+    for i, v in vals:
+        r[int(i)] = float(v)
+    return r, t
+
+
+def ref_spmv(path: str, iters: int, threads=None, result=True, timeout=600):
+    """numa-SPMV <weighted text> <iters> [-result]; returns (x|None, seconds)."""
+    args = [os.path.join(REF_DIR, "numa-SPMV"), path, str(iters), "-result" if result else "-noresult"]
+    out, t = _run(args, threads, timeout)
+    if not result:
+        return None, t
+    vals = re.findall(r"^(\d+)\t([0-9.eE+-]+)$", out, re.M)
+    r = np.zeros(len(vals), np.float64)
+    for i, v in vals:
+        r[int(i)] = float(v)
+    return r, t
+
+
+def ref_components(path: str, binary: bool = True, threads=None, result=True, timeout=600):
+    """numa-Components <g> -s [-result] [-b]; returns (labels|None, seconds)."""
+    args = [os.path.join(REF_DIR, "numa-Components"), path, "-s",
+            "-result" if result else "-noresult", "-b" if binary else "-t"]
+    out, t = _run(args, threads, timeout)
+    if not result:
+        return None, t
+    vals = re.findall(r"^Result of (\d+) : (-?\d+)$", out, re.M)
+    r = np.zeros(len(vals), np.int32)
+    for i, v in vals:
+        r[int(i)] = int(v)
+    return r, t
+
+
+def ref_bfs(path: str, src: int, binary: bool = True, symmetric: bool = True, threads=None,
+            parents=True, timeout=600):
+    """numa-BFS (or the parent-printing build) <g> <src> -result [-s] [-b];
+    returns (parents|None, visited count, seconds)."""
+    exe = "numa-BFS-parents" if parents else "numa-BFS"
+    args = [os.path.join(REF_DIR, exe), path, str(src), "-result",
+            "-s" if symmetric else "-a", "-b" if binary else "-t"]
+    out, t = _run(args, threads, timeout)
+    cnt = re.findall(r"^Vert visited: (\d+)", out, re.M)
+    par = None
+    if parents:
+        vals = re.findall(r"^parent (\d+) (-?\d+)$", out, re.M)
+        par = np.full(len(vals), -1, np.int32)
+        for i, v in vals:
+            par[int(i)] = int(v)
+    return par, (int(cnt[-1]) if cnt else -1), t
+
+
+def ref_bellman_ford(path: str, src: int, threads=None, result=False, timeout=600):
+    """numa-BellmanFord(-dist) <weighted text> <src> [-result] -s."""
+    exe = "numa-BellmanFord-dist" if result else "numa-BellmanFord"
+    args = [os.path.join(REF_DIR, exe), path, str(src), "-result" if result else "-noresult", "-s"]
+    out, t = _run(args, threads, timeout)
+    if not result:
+        return None, t
+    vals = re.findall(r"^(\d+)\t(-?\d+)$", out, re.M)
+    r = np.zeros(len(vals), np.int32)
+    for i, v in vals:
+        r[int(i)] = int(v)
+    return r, t
+
+
+def ref_bp(path: str, iters: int, binary: bool = True, threads=None, timeout=600):
+    """numa-BP <g> <iters> (the reference prints no result); returns seconds."""
+    args = [os.path.join(REF_DIR, "numa-BP"), path, str(iters), "-noresult", "-a",
+            "-b" if binary else "-t"]
+    _, t = _run(args, threads, timeout)
+    return t
+
+
+def tempdir() -> str:
+    return tempfile.mkdtemp(prefix="pm_oracle_")

@@ -1,0 +1,344 @@
+"""polymer_b200 -- Python binding of the B200 edgeMap/vertexMap engine.
+
+The engine is libpolymer_b200.so (CUDA kernels for sm_100a behind the C ABI
+in include/polymer_b200.h).  This module is a thin ctypes layer over that
+ABI, named after the reference applications it replaces:
+
+    g = Graph.from_csr(offsets, edges)            # readGraph (IO-numa.h:745)
+    ranks = PageRank(g, maxIter=10)                # numa-PageRank.C:548
+    parents, depth = BFS(src, g)                   # numa-BFS.C:476
+    labels = Components(g)                         # numa-Components.C:402
+    dist = BellmanFord(g, src)                     # numa-BellmanFord.C:400
+    y = SPMV(g, x0, maxIter)                       # numa-SPMV.C:335
+    logp = BeliefPropagation(g, prior, maxIter)    # numa-BP.C:528
+
+Arrays are numpy (host) or any object exposing a CUDA pointer through
+``data_ptr()`` (torch tensors).  There is no CPU fallback: without the
+shared library or a GPU every call raises PolymerError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = [
+    "Graph", "PolymerError", "PageRank", "BFS", "Components", "BellmanFord", "SPMV",
+    "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
+]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_b200.so")
+
+PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
+PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS = 2, 4
+PM_F32, PM_F64 = 0, 1
+BF_INF = 1073741823
+
+_STATUS = {
+    0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "TIMEOUT", 5: "BAD_GRAPH",
+    6: "NOT_SUPPORTED", 7: "NO_DEVICE",
+}
+
+
+class PolymerError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s: %s" % (_STATUS.get(status, status), msg))
+        self.status = status
+
+
+class TraversalStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("dense_rounds", C.c_int32),
+                ("edges_visited", C.c_int64), ("reached", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine; raises PolymerError when it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PolymerError(6, "libpolymer_b200.so is not built (run polymer_b200/_build.py)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, u32, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64
+    sigs = {
+        "pm_graph_create": [vp, vp, i64, i64, u32, u32, C.c_int, C.POINTER(vp)],
+        "pm_graph_create_rmat": [C.c_int, C.c_int, u64, u32, C.c_int, C.POINTER(vp)],
+        "pm_graph_destroy": [vp],
+        "pm_graph_info": [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)],
+        "pm_graph_get_csr": [vp, vp, vp, u32],
+        "pm_graph_set_weights_i32": [vp, vp, u32],
+        "pm_graph_set_weights_f32": [vp, vp, u32],
+        "pm_graph_gen_weights_i32": [vp, u64, i32],
+        "pm_graph_gen_weights_f32": [vp, u64],
+        "pm_graph_get_weights_f32": [vp, vp, u32],
+        "pm_graph_get_weights_i32": [vp, vp, u32],
+        "pm_fill_uniform_f32": [vp, u64, C.c_int, vp, i64],
+        "pm_bfs": [vp, i32, vp, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_components": [vp, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
+        "pm_spmv": [vp, vp, C.c_int, vp, u32, vp],
+        "pm_bp": [vp, vp, vp, C.c_int, vp, u32],
+        "pm_timer_begin": [vp],
+        "pm_timer_end": [vp, C.POINTER(C.c_float)],
+        "pm_profile_enable": [vp, C.c_int],
+        "pm_profile_read": [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(i64), C.c_int],
+        "pm_host_alloc": [u64, C.POINTER(vp)],
+        "pm_host_free": [vp],
+    }
+    for name, args in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.pm_kernel_launches.argtypes = [C.c_int]
+    L.pm_kernel_launches.restype = C.c_int64
+    L.pm_last_error.restype = C.c_char_p
+    L.pm_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise PolymerError(status, lib().pm_last_error().decode(errors="replace"))
+
+
+def kernel_launches(reset: bool = False) -> int:
+    return int(lib().pm_kernel_launches(int(reset)))
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
+
+
+def _arg(a, dtype):
+    """(pointer, mem flag, keep-alive) for a numpy array or CUDA tensor."""
+    if a is None:
+        return None, PM_MEM_HOST, None
+    if _is_device(a):
+        return C.c_void_p(a.data_ptr()), PM_MEM_DEVICE, a
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data_as(C.c_void_p), PM_MEM_HOST, arr
+
+
+class Graph:
+    """A graph resident on one GPU (CSR + CSC, int32 ids and offsets)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        n, m, md = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(lib().pm_graph_info(self._h, C.byref(n), C.byref(m), C.byref(md)))
+        self.n, self.m, self.max_out_degree = n.value, m.value, md.value
+
+    @classmethod
+    def from_csr(cls, offsets, edges, symmetric: bool = False, skip_self_loops: bool = False,
+                 device: int = 0) -> "Graph":
+        """offsets: n+1 int32 (offsets[n] == m); edges: m int32 destinations."""
+        n = len(offsets) - 1
+        m = len(edges)
+        po, mem, ko = _arg(offsets, np.int32)
+        pe, mem2, ke = _arg(edges, np.int32)
+        if mem != mem2:
+            raise PolymerError(1, "offsets and edges must live in the same memory space")
+        flags = (PM_GRAPH_SYMMETRIC if symmetric else 0) | (PM_GRAPH_SKIP_SELF_LOOPS if skip_self_loops else 0)
+        h = C.c_void_p()
+        _check(lib().pm_graph_create(po, pe, n, m, flags, mem, device, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_pbbs(cls, offsets_n, edges, **kw) -> "Graph":
+        """PBBS AdjacencyGraph arrays: n offsets (no trailing m) and m edges."""
+        off = np.append(np.ascontiguousarray(offsets_n, np.int32), np.int32(len(edges)))
+        return cls.from_csr(off, np.ascontiguousarray(edges, np.int32), **kw)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 0x5EED0001, symmetric: bool = False,
+             device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().pm_graph_create_rmat(scale, edge_factor, seed,
+                                          PM_GRAPH_SYMMETRIC if symmetric else 0, device, C.byref(h)))
+        return cls(h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pm_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def csr(self):
+        off = np.empty(self.n + 1, np.int32)
+        idx = np.empty(max(self.m, 1), np.int32)
+        _check(lib().pm_graph_get_csr(self._h, off.ctypes.data_as(C.c_void_p),
+                                      idx.ctypes.data_as(C.c_void_p), PM_MEM_HOST))
+        return off, idx[: self.m]
+
+    def set_weights(self, w) -> None:
+        """int32 weights (BellmanFord) or float32 weights (SpMV), CSR order."""
+        is_float = (np.asarray(w).dtype.kind == "f") if not _is_device(w) else w.is_floating_point()
+        p, mem, keep = _arg(w, np.float32 if is_float else np.int32)
+        fn = lib().pm_graph_set_weights_f32 if is_float else lib().pm_graph_set_weights_i32
+        _check(fn(self._h, p, mem))
+
+    def gen_weights_int(self, seed: int = 0x5EED0002, wmax: int = 22) -> None:
+        _check(lib().pm_graph_gen_weights_i32(self._h, seed, wmax))
+
+    def gen_weights_unit(self, seed: int = 0x5EED0002) -> None:
+        _check(lib().pm_graph_gen_weights_f32(self._h, seed))
+
+    def weights_f32(self) -> np.ndarray:
+        w = np.empty(max(self.m, 1), np.float32)
+        _check(lib().pm_graph_get_weights_f32(self._h, w.ctypes.data_as(C.c_void_p), PM_MEM_HOST))
+        return w[: self.m]
+
+    def weights_i32(self) -> np.ndarray:
+        w = np.empty(max(self.m, 1), np.int32)
+        _check(lib().pm_graph_get_weights_i32(self._h, w.ctypes.data_as(C.c_void_p), PM_MEM_HOST))
+        return w[: self.m]
+
+    def timer_begin(self) -> None:
+        _check(lib().pm_timer_begin(self._h))
+
+    def timer_end(self) -> float:
+        ms = C.c_float()
+        _check(lib().pm_timer_end(self._h, C.byref(ms)))
+        return ms.value
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().pm_profile_enable(self._h, int(enable)))
+
+    def profile_read(self, tag: str, reset: bool = False):
+        """(total device ms, number of passes) recorded under tag."""
+        ms, cnt = C.c_double(), C.c_int64()
+        _check(lib().pm_profile_read(self._h, tag.encode(), C.byref(ms), C.byref(cnt), int(reset)))
+        return ms.value, cnt.value
+
+
+class PinnedArray:
+    """A numpy view of page-locked host memory from pm_host_alloc."""
+
+    def __init__(self, count: int, dtype):
+        self.dtype = np.dtype(dtype)
+        self._p = C.c_void_p()
+        _check(lib().pm_host_alloc(max(count, 1) * self.dtype.itemsize, C.byref(self._p)))
+        buf = (C.c_char * (max(count, 1) * self.dtype.itemsize)).from_address(self._p.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=count)
+
+    def free(self) -> None:
+        if self._p:
+            self.array = None
+            lib().pm_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _out(like, n, dtype):
+    """Output buffer in the memory space of `like` (torch CUDA tensor) or numpy."""
+    if like is not None and _is_device(like):
+        import torch
+        t = torch.empty(n, dtype={np.int32: torch.int32, np.float32: torch.float32,
+                                  np.float64: torch.float64}[dtype], device=like.device)
+        return t, C.c_void_p(t.data_ptr()), PM_MEM_DEVICE
+    a = np.empty(max(n, 1), dtype)[:n]
+    return a, a.ctypes.data_as(C.c_void_p), PM_MEM_HOST
+
+
+def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool = False):
+    """Parents and depths from `start` (numa-BFS.C BFS_F).  threshold < 0:
+    direction switch at m/20; 0: dense pull every level as the reference."""
+    par, pp, mem = _out(device_out, g.n, np.int32)
+    dep, pd, _ = _out(device_out, g.n, np.int32)
+    st = TraversalStats()
+    _check(lib().pm_bfs(g.handle, int(start), pp, pd, mem, int(threshold), C.byref(st)))
+    return (par, dep, st.as_dict()) if stats else (par, dep)
+
+
+def Components(g: Graph, threshold: int = -1, device_out=None, stats: bool = False):
+    """Min-label connected components (numa-Components.C CC_F)."""
+    lab, pl, mem = _out(device_out, g.n, np.int32)
+    st = TraversalStats()
+    _check(lib().pm_components(g.handle, pl, mem, int(threshold), C.byref(st)))
+    return (lab, st.as_dict()) if stats else lab
+
+
+def BellmanFord(g: Graph, start: int, threshold: int = -1, device_out=None, stats: bool = False):
+    """Shortest-path distances over the int32 weights (numa-BellmanFord.C BF_F)."""
+    dist, pd, mem = _out(device_out, g.n, np.int32)
+    st = TraversalStats()
+    _check(lib().pm_bellman_ford(g.handle, int(start), pd, mem, int(threshold), C.byref(st)))
+    return (dist, st.as_dict()) if stats else dist
+
+
+def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float64,
+             device_out=None, resid: bool = False):
+    """Polymer-semantics PageRank (numa-PageRank.C PR_F); dtype float32/float64."""
+    dt = np.float64 if np.dtype(dtype) == np.float64 else np.float32
+    ranks, pr, mem = _out(device_out, g.n, dt)
+    res = np.zeros(max(maxIter, 1), np.float64)
+    _check(lib().pm_pagerank(g.handle, int(maxIter), float(damping),
+                             PM_F64 if dt == np.float64 else PM_F32, pr, mem,
+                             res.ctypes.data_as(C.c_void_p) if resid else None))
+    return (ranks, res[:maxIter]) if resid else ranks
+
+
+def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False):
+    """x <- A_w^T x, maxIter times, over the float weights (numa-SPMV.C SPMV_F)."""
+    px, mem, keep = _arg(x0, np.float32)
+    y, py, _ = _out(x0 if mem == PM_MEM_DEVICE else None, g.n, np.float32)
+    nrm = np.zeros(max(maxIter, 1), np.float64)
+    _check(lib().pm_spmv(g.handle, px, int(maxIter), py, mem,
+                         nrm.ctypes.data_as(C.c_void_p) if norms else None))
+    return (y, nrm[:maxIter]) if norms else y
+
+
+def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1, 0.9))):
+    """2-state BP log-products (n x 2) (numa-BP.C BP_F, normalised messages)."""
+    pp, mem, keep = _arg(prior, np.float32)
+    psi_a = np.ascontiguousarray(psi, np.float32).reshape(4)
+    if mem == PM_MEM_DEVICE:
+        import torch
+        psi_t = torch.tensor(psi_a, device=prior.device)
+        ppsi = C.c_void_p(psi_t.data_ptr())
+    else:
+        psi_t = psi_a
+        ppsi = psi_a.ctypes.data_as(C.c_void_p)
+    out, po, _ = _out(prior if mem == PM_MEM_DEVICE else None, 2 * g.n, np.float32)
+    _check(lib().pm_bp(g.handle, pp, ppsi, int(maxIter), po, mem))
+    return out.reshape(g.n, 2)
+
+
+def uniform_f32(g: Graph, count: int, seed: int, open_interval: bool = False):
+    """Seeded uniform floats on g's device ([0,1), or (0,1) with open_interval),
+    the oracle's pmo_fill_uniform01 / _open rule; returns a torch CUDA tensor."""
+    import torch
+    x = torch.empty(count, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    _check(lib().pm_fill_uniform_f32(g.handle, seed, int(open_interval), C.c_void_p(x.data_ptr()),
+                                     count))
+    return x

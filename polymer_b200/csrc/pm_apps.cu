@@ -1,0 +1,361 @@
+// pm_apps.cu -- the six Polymer applications as host loops over the engine.
+//
+// Each app keeps the reference's functor (cond / updateAtomic for pushes,
+// identity / edge / combine / commit for the reducing pull, with the
+// application's vertexMap fused into commit) and its iteration loop, with
+// the NUMA worker/sub-worker scaffolding replaced by kernel launches on the
+// graph's stream.
+#include <cmath>
+#include <cstring>
+
+#include "pm_graph.cuh"
+
+namespace pm {
+
+// ===========================================================================
+// BFS  (numa-BFS.C:59-79 BFS_F, loop 258-296)
+// ===========================================================================
+struct BFS_F {
+  int32_t *parents;
+  int32_t *depth;
+  int32_t level;
+  // cond: not visited yet
+  __device__ __forceinline__ bool cond(int d) const {
+    return *((volatile int32_t *)parents + d) == -1;
+  }
+  // updateAtomic: CAS(Parents[d], -1, s)
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int) const {
+    if (atomicCAS(parents + d, -1, s) == -1) {
+      depth[d] = level;
+      return true;
+    }
+    return false;
+  }
+};
+
+__global__ void k_bfs_init(int32_t *parents, int32_t *depth, int64_t n, int32_t src) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    parents[v] = v == src ? src : -1;
+    depth[v] = v == src ? 0 : -1;
+  }
+}
+
+void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
+             pm_traversal_stats *st) {
+  Engine &E = g->E;
+  VertexSubset cur = g->subset(0), next = g->subset(1);
+  PM_LAUNCH(k_bfs_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_parents, d_depth, g->n, src);
+  subset_single(E, cur, src);
+  pm_traversal_stats s{};
+  s.reached = 1;
+  E.tag = "bfs";
+  for (int32_t level = 1; cur.size > 0; ++level) {
+    bool dense = false;
+    s.edges_visited += cur.edges;
+    edgeMap<int>(E, cur, BFS_F{d_parents, d_depth, level}, next, threshold, DENSE_PARALLEL, nullptr,
+                 nullptr, &dense);
+    s.rounds++;
+    s.dense_rounds += dense;
+    s.reached += next.size;
+    std::swap(cur, next);
+  }
+  if (st) *st = s;
+}
+
+// ===========================================================================
+// Connected components  (numa-Components.C:55-119 CC_F / CC_Vertex_F,
+// loop 233-281, edgeMapCustom 121-175)
+// The reference activates d when writeMin(IDs[d], IDs[s]) succeeds while
+// IDs[d] still equals prevIDs[d]; prevIDs equals IDs for every vertex at the
+// start of a round, so that is "the first lowering of d in this round" --
+// here the dedup bit of the next frontier.  The result is the same.
+// ===========================================================================
+struct CC_F {
+  int32_t *ids;
+  const uint32_t *cur;
+  using Acc = int32_t;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int) const {
+    int32_t v = *((volatile int32_t *)ids + s);
+    return v < atomicMin(ids + d, v);
+  }
+  __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
+  __device__ __forceinline__ Acc edge(int s, int, int) const {
+    return test_bit(cur, s) ? *((volatile int32_t *)ids + s) : 0x7fffffff;
+  }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return min(a, b); }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double &) const {
+    if (acc < ids[d]) {
+      ids[d] = acc;
+      return true;
+    }
+    return false;
+  }
+};
+
+__global__ void k_iota32(int32_t *a, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) a[v] = (int32_t)v;
+}
+
+void run_cc(pm_graph *g, int32_t *d_labels, int64_t threshold, pm_traversal_stats *st) {
+  Engine &E = g->E;
+  VertexSubset cur = g->subset(0), next = g->subset(1);
+  PM_LAUNCH(k_iota32, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_labels, g->n);
+  subset_all(E, cur);
+  pm_traversal_stats s{};
+  E.tag = "cc";
+  while (cur.size > 0) {
+    bool dense = false;
+    s.edges_visited += cur.edges;
+    edgeMapReduce<int>(E, cur, CC_F{d_labels, cur.bits}, next, threshold, nullptr, nullptr, &dense);
+    s.rounds++;
+    s.dense_rounds += dense;
+    std::swap(cur, next);
+  }
+  s.reached = g->n;
+  if (st) *st = s;
+}
+
+// ===========================================================================
+// BellmanFord  (numa-BellmanFord.C:61-95 BF_F / BF_Vertex_F, loop 166-211)
+// Next frontier = vertices whose distance fell this round (Ligra's reset of
+// Visited on the output; the reference resets on the current frontier,
+// which can lose re-improved vertices).  Dense rounds pull min(dist[s] + w)
+// over the CSC instead of pushing writeMin over the CSR; both compute the
+// same round result.
+// ===========================================================================
+struct BF_F {
+  int32_t *dist;
+  const uint32_t *cur;
+  using Acc = int32_t;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int32_t w) const {
+    int32_t nd = *((volatile int32_t *)dist + s) + w;
+    return nd < atomicMin(dist + d, nd);
+  }
+  __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
+  __device__ __forceinline__ Acc edge(int s, int, int32_t w) const {
+    return test_bit(cur, s) ? *((volatile int32_t *)dist + s) + w : 0x7fffffff;
+  }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return min(a, b); }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double &) const {
+    if (acc < dist[d]) {
+      dist[d] = acc;
+      return true;
+    }
+    return false;
+  }
+};
+
+__global__ void k_bf_init(int32_t *dist, int64_t n, int32_t src) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+    dist[v] = v == src ? 0 : kDevBFInf;
+}
+
+void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t threshold,
+                      pm_traversal_stats *st) {
+  Engine &E = g->E;
+  VertexSubset cur = g->subset(0), next = g->subset(1);
+  PM_LAUNCH(k_bf_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_dist, g->n, src);
+  subset_single(E, cur, src);
+  pm_traversal_stats s{};
+  s.reached = 1;
+  const int32_t *w_out = g->w_i32_out.as<int32_t>(), *w_in = g->w_i32_in.as<int32_t>();
+  E.tag = "bellman_ford";
+  while (cur.size > 0) {
+    bool dense = false;
+    s.edges_visited += cur.edges;
+    edgeMapReduce<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, w_out, w_in, &dense);
+    s.rounds++;
+    s.dense_rounds += dense;
+    std::swap(cur, next);
+    if (s.rounds > g->n + 1) fail(PM_ERR_INVALID_ARG, "BellmanFord did not converge");
+  }
+  if (st) *st = s;
+}
+
+// ===========================================================================
+// PageRank  (numa-PageRank.C:64-148 PR_F / PR_Vertex_F / PR_Vertex_Reset,
+// loop 273-335)
+// One pull-reduce per iteration.  The frontier rides in the contribution
+// array: c[s] = p[s] / outdeg(s) when s is in the frontier (>= +0), and
+// -0.0 when it is not.  -0.0 is the exact additive identity, so the sum of
+// a row's contributions is -0.0 exactly when no in-neighbour is in the
+// frontier: its sign bit is the next-frontier bit.  commit() applies the
+// push sum to the stale p_next, damps frontier vertices (PR_Vertex_F),
+// zeroes their p_curr (PR_Vertex_Reset) and writes next round's
+// contribution; the FP64 L1 residual is reduced on the side.
+// ===========================================================================
+template <class T>
+struct PR_F {
+  const T *c_cur;
+  T *c_next;
+  T *pc;
+  T *pn;
+  const int32_t *out_off;
+  T damping, added;
+  using Acc = T;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ Acc identity() const { return T(-0.0); }
+  __device__ __forceinline__ Acc edge(int s, int, int) const { return __ldg(c_cur + s); }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double &resid) const {
+    const bool in_f = !signbit(__ldg(c_cur + d));
+    const bool hit = !signbit(acc);
+    const T old = pc[d];
+    T nb = pn[d] + acc;
+    if (in_f) {
+      nb = damping * nb + added;
+      pc[d] = T(0);
+    }
+    pn[d] = nb;
+    const int deg = __ldg(out_off + d + 1) - __ldg(out_off + d);
+    c_next[d] = hit ? (deg > 0 ? nb / T(deg) : T(0)) : T(-0.0);
+    resid += fabs((double)nb - (double)old);
+    return hit;
+  }
+};
+
+template <class T>
+__global__ void k_pr_init(T *pc, T *pn, T *c, const int32_t *out_off, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const T p0 = T(1) / T(n);
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    pc[v] = p0;
+    pn[v] = T(0);
+    int deg = out_off[v + 1] - out_off[v];
+    c[v] = deg > 0 ? p0 / T(deg) : T(0);
+  }
+}
+
+__global__ void k_copy_daux(const Counters *cnt, double *dst) { *dst = cnt->daux; }
+
+template <class T>
+void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  T *pc = (T *)g->scratch_buf(0, (size_t)n * sizeof(T));
+  T *pn = (T *)g->scratch_buf(1, (size_t)n * sizeof(T));
+  T *c0 = (T *)g->scratch_buf(2, (size_t)n * sizeof(T));
+  T *c1 = (T *)g->scratch_buf(3, (size_t)n * sizeof(T));
+  PM_LAUNCH((k_pr_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, pc, pn, c0, E.g.out.off, n);
+  const T dmp = (T)damping, added = (T)((1.0 - damping) * (1.0 / (double)n));
+  for (int it = 0; it < iters; ++it) {
+    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+    E.prof.begin("pagerank", E.stream);
+    launch_pull_reduce<int>(E, PR_F<T>{c0, c1, pc, pn, E.g.out.off, dmp, added}, nullptr, nullptr,
+                            E.d_cnt);
+    E.prof.end(E.stream);
+    if (d_resid) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_resid + it);
+    std::swap(pc, pn);
+    std::swap(c0, c1);
+  }
+  PM_CUDA(cudaMemcpyAsync(d_out, pc, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
+}
+
+// ===========================================================================
+// SpMV  (numa-SPMV.C:56-110 SPMV_F / SPMV_Vertex_Reset, loop 168-193)
+// All vertices are active every iteration: y[d] = sum w(s,d) x[s] as a
+// pull over the CSC with the weights permuted to CSC order; x <- y.
+// ===========================================================================
+struct SPMV_F {
+  const float *x;
+  float *y;
+  using Acc = float;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ Acc identity() const { return -0.0f; }
+  __device__ __forceinline__ Acc edge(int s, int, float w) const { return w * __ldg(x + s); }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double &norm) const {
+    const float v = acc + 0.0f;
+    y[d] = v;
+    norm += fabs((double)v);
+    return false;
+  }
+};
+
+void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  float *x = (float *)g->scratch_buf(0, (size_t)n * 4);
+  float *y = (float *)g->scratch_buf(1, (size_t)n * 4);
+  PM_CUDA(cudaMemcpyAsync(x, d_x0, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+  const float *w_in = g->w_f32_in.as<float>();
+  for (int it = 0; it < iters; ++it) {
+    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+    E.prof.begin("spmv", E.stream);
+    launch_pull_reduce<float>(E, SPMV_F{x, y}, w_in, nullptr, E.d_cnt);
+    E.prof.end(E.stream);
+    if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
+    std::swap(x, y);
+  }
+  PM_CUDA(cudaMemcpyAsync(d_y, x, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+}
+
+// ===========================================================================
+// Belief propagation, 2 states  (numa-BP.C:89-140 BP_F / BP_Vertex_Reset,
+// edgeMapDenseBPNoRep 179-230, loop 280-316)
+// With one psi for every edge the message of an edge s->d depends on d
+// alone, so prod'_d *= belief_d ^ k_d where k_d counts d's in-neighbours in
+// the frontier: the pull reduces k_d and commit() applies it, in logs.
+// Messages are normalised to sum 1 (see pm_bp in the header).
+// ===========================================================================
+struct BP_F {
+  const uint32_t *cur;
+  const float2 *lc;
+  float2 *ln;
+  const float2 *prior;
+  float p00, p01, p10, p11;
+  using Acc = int32_t;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ Acc identity() const { return 0; }
+  __device__ __forceinline__ Acc edge(int s, int, int) const { return test_bit(cur, s) ? 1 : 0; }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
+  __device__ __forceinline__ bool commit(int d, Acc k, double &) const {
+    const bool in_f = test_bit(cur, d);
+    float2 out = in_f ? make_float2(0.f, 0.f) : ln[d];
+    if (k > 0) {
+      const float2 l = lc[d], pr = prior[d];
+      const float lm = fmaxf(l.x, l.y);
+      const float a0 = pr.x * expf(l.x - lm), a1 = pr.y * expf(l.y - lm);
+      const float b0 = p00 * a0 + p01 * a1, b1 = p10 * a0 + p11 * a1;
+      const float lz = logf(b0 + b1);
+      out.x += (float)k * (logf(b0) - lz);
+      out.y += (float)k * (logf(b1) - lz);
+    }
+    if (in_f || k > 0) ln[d] = out;
+    return k > 0;
+  }
+};
+
+void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  float2 *lc = (float2 *)g->scratch_buf(0, (size_t)n * 8);
+  float2 *ln = (float2 *)g->scratch_buf(1, (size_t)n * 8);
+  PM_CUDA(cudaMemsetAsync(lc, 0, (size_t)n * 8, E.stream));
+  PM_CUDA(cudaMemsetAsync(ln, 0, (size_t)n * 8, E.stream));
+  VertexSubset cur = g->subset(0), next = g->subset(1);
+  subset_all(E, cur);
+  for (int it = 0; it < iters; ++it) {
+    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+    E.prof.begin("bp", E.stream);
+    launch_pull_reduce<int>(E,
+                            BP_F{cur.bits, lc, ln, (const float2 *)d_prior, psi[0], psi[1], psi[2],
+                                 psi[3]},
+                            nullptr, next.bits, E.d_cnt);
+    E.prof.end(E.stream);
+    std::swap(lc, ln);
+    std::swap(cur, next);
+  }
+  PM_CUDA(cudaMemcpyAsync(d_out, lc, (size_t)n * 8, cudaMemcpyDeviceToDevice, E.stream));
+}
+
+// explicit instantiations used by the C ABI
+template void run_pagerank<float>(pm_graph *, int, double, float *, double *);
+template void run_pagerank<double>(pm_graph *, int, double, double *, double *);
+
+}  // namespace pm

@@ -1,0 +1,438 @@
+// pm_capi.cu -- the extern "C" boundary (include/polymer_b200.h).
+// Every entry point validates its arguments, stages host arrays through the
+// handle's device scratch, runs on the graph's stream and converts internal
+// failures into a pm_status plus a thread-local message.
+#include <cstdio>
+#include <cstring>
+
+#include "pm_graph.cuh"
+
+namespace pm {
+long long launches(bool reset);
+void ingest_csr(pm_graph *g, bool skip_self_loops);
+void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed);
+void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float);
+void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count);
+void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
+             pm_traversal_stats *st);
+void run_cc(pm_graph *g, int32_t *d_labels, int64_t threshold, pm_traversal_stats *st);
+void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t threshold,
+                      pm_traversal_stats *st);
+template <class T>
+void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid);
+void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm);
+void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
+}  // namespace pm
+
+using namespace pm;
+
+static thread_local std::string t_last_error;
+
+// Scratch slots used for staging at the boundary (the algorithms use 0..3).
+enum { kSlotIn0 = 8, kSlotIn1 = 9, kSlotOut0 = 10, kSlotOut1 = 11, kSlotAux = 12 };
+
+template <class Fn>
+static pm_status guard(Fn &&fn) {
+  try {
+    fn();
+    t_last_error.clear();
+    return PM_OK;
+  } catch (const Failure &f) {
+    t_last_error = f.what();
+    return f.status;
+  } catch (const std::bad_alloc &) {
+    t_last_error = "host allocation failed";
+    return PM_ERR_OOM;
+  } catch (const std::exception &e) {
+    t_last_error = e.what();
+    return PM_ERR_CUDA;
+  }
+}
+
+static void need(bool ok, const char *msg) {
+  if (!ok) fail(PM_ERR_INVALID_ARG, msg);
+}
+
+static void use_device(int dev) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    (void)cudaGetLastError();
+    fail(PM_ERR_NO_DEVICE, "no CUDA device visible");
+  }
+  need(dev >= 0 && dev < count, "device index out of range");
+  PM_CUDA(cudaSetDevice(dev));
+}
+
+static pm_graph *new_graph(int device, bool symmetric) {
+  use_device(device);
+  auto *g = new pm_graph();
+  g->device = device;
+  g->symmetric = symmetric;
+  try {
+    PM_CUDA(cudaStreamCreateWithFlags(&g->E.stream, cudaStreamNonBlocking));
+    PM_CUDA(cudaMallocHost(&g->h_cnt, 3 * sizeof(Counters)));
+    g->E.h_cnt = g->h_cnt;
+    PM_CUDA(cudaEventCreate(&g->ev0));
+    PM_CUDA(cudaEventCreate(&g->ev1));
+    PM_CUDA(cudaDeviceGetAttribute(&g->E.num_sms, cudaDevAttrMultiProcessorCount, device));
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  return g;
+}
+
+// Copy count elements between host/device and a device buffer on the stream.
+static void to_device(pm_graph *g, void *dst, const void *src, size_t bytes, uint32_t mem) {
+  if (bytes == 0) return;
+  PM_CUDA(cudaMemcpyAsync(dst, src, bytes,
+                          mem == PM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                          g->E.stream));
+}
+static void from_device(pm_graph *g, void *dst, const void *src, size_t bytes, uint32_t mem) {
+  if (bytes == 0) return;
+  PM_CUDA(cudaMemcpyAsync(dst, src, bytes,
+                          mem == PM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                          g->E.stream));
+}
+static void finish(pm_graph *g) { PM_CUDA(cudaStreamSynchronize(g->E.stream)); }
+static void check_mem(uint32_t mem) { need(mem == PM_MEM_HOST || mem == PM_MEM_DEVICE, "mem must be PM_MEM_HOST or PM_MEM_DEVICE"); }
+static void enter(pm_graph *g) {
+  need(g != nullptr, "null graph handle");
+  PM_CUDA(cudaSetDevice(g->device));
+}
+
+extern "C" {
+
+pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t n, int64_t m,
+                          uint32_t flags, uint32_t mem, int device, pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
+    need(m >= 0 && m < (1ll << 31) - 1, "m must be in [0, 2^31-2]");
+    need(offsets != nullptr && (m == 0 || edges != nullptr), "null offsets/edges");
+    check_mem(mem);
+    pm_graph *g = new_graph(device, (flags & PM_GRAPH_SYMMETRIC) != 0);
+    try {
+      g->n = n;
+      g->m = m;
+      g->out.off.alloc((size_t)(n + 1) * 4);
+      g->out.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+      to_device(g, g->out.off.p, offsets, (size_t)(n + 1) * 4, mem);
+      to_device(g, g->out.idx.p, edges, (size_t)m * 4, mem);
+      ingest_csr(g, (flags & PM_GRAPH_SKIP_SELF_LOOPS) != 0);
+      finish_graph(g);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32_t flags, int device,
+                               pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(scale >= 1 && scale <= 28, "scale must be in [1, 28]");
+    need(edge_factor >= 1 && edge_factor <= 64, "edge_factor must be in [1, 64]");
+    need(((int64_t)edge_factor << scale) * ((flags & PM_GRAPH_SYMMETRIC) ? 2 : 1) < (1ll << 31) - 1,
+         "graph exceeds int32 edge offsets");
+    pm_graph *g = new_graph(device, (flags & PM_GRAPH_SYMMETRIC) != 0);
+    try {
+      generate_rmat(g, scale, edge_factor, seed);
+      finish_graph(g);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+pm_status pm_graph_destroy(pm_graph *g) {
+  return guard([&] {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    delete g;
+  });
+}
+
+pm_status pm_graph_info(const pm_graph *g, int64_t *n, int64_t *m, int64_t *max_out_degree) {
+  return guard([&] {
+    need(g != nullptr, "null graph handle");
+    if (n) *n = g->n;
+    if (m) *m = g->m;
+    if (max_out_degree) *max_out_degree = g->max_out_deg;
+  });
+}
+
+pm_status pm_graph_get_csr(pm_graph *g, int32_t *offsets, int32_t *edges, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    if (offsets) from_device(g, offsets, g->out.off.p, (size_t)(g->n + 1) * 4, mem);
+    if (edges) from_device(g, edges, g->out.idx.p, (size_t)g->m * 4, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(w != nullptr || g->m == 0, "null weights");
+    g->w_i32_out.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
+    to_device(g, g->w_i32_out.p, w, (size_t)g->m * 4, mem);
+    permute_weights_i32(g);
+  });
+}
+
+pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(w != nullptr || g->m == 0, "null weights");
+    g->w_f32_out.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
+    to_device(g, g->w_f32_out.p, w, (size_t)g->m * 4, mem);
+    permute_weights_f32(g);
+  });
+}
+
+pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax) {
+  return guard([&] {
+    enter(g);
+    need(wmax >= 1, "wmax must be >= 1");
+    gen_weights(g, seed, wmax, false);
+  });
+}
+
+pm_status pm_graph_gen_weights_f32(pm_graph *g, uint64_t seed) {
+  return guard([&] {
+    enter(g);
+    gen_weights(g, seed, 0, true);
+  });
+}
+
+pm_status pm_graph_get_weights_f32(pm_graph *g, float *w, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(g->w_f32_out.p != nullptr, "graph has no float weights");
+    from_device(g, w, g->w_f32_out.p, (size_t)g->m * 4, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_graph_get_weights_i32(pm_graph *g, int32_t *w, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(g->w_i32_out.p != nullptr, "graph has no int weights");
+    from_device(g, w, g->w_i32_out.p, (size_t)g->m * 4, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_fill_uniform_f32(pm_graph *g, uint64_t seed, int open_interval, float *out,
+                              int64_t count) {
+  return guard([&] {
+    enter(g);
+    need(out != nullptr && count >= 0, "bad output");
+    fill_uniform(g, seed, open_interval, out, count);
+  });
+}
+
+pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
+                 int64_t threshold, pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(src >= 0 && src < g->n, "source out of range");
+    const size_t bytes = (size_t)g->n * 4;
+    int32_t *dp = (int32_t *)g->scratch_buf(kSlotOut0, bytes);
+    int32_t *dd = (int32_t *)g->scratch_buf(kSlotOut1, bytes);
+    run_bfs(g, src, dp, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    if (parents) from_device(g, parents, dp, bytes, mem);
+    if (depth) from_device(g, depth, dd, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t threshold,
+                        pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(labels != nullptr, "null labels");
+    const size_t bytes = (size_t)g->n * 4;
+    int32_t *dl = mem == PM_MEM_DEVICE ? labels : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
+    run_cc(g, dl, threshold < 0 ? g->m / 8 : threshold, stats);
+    if (mem == PM_MEM_HOST) from_device(g, labels, dl, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem, int64_t threshold,
+                          pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(dist != nullptr, "null dist");
+    need(src >= 0 && src < g->n, "source out of range");
+    need(g->w_i32_out.p != nullptr, "graph has no int32 weights (pm_graph_set_weights_i32)");
+    const size_t bytes = (size_t)g->n * 4;
+    int32_t *dd = mem == PM_MEM_DEVICE ? dist : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
+    run_bellman_ford(g, src, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    if (mem == PM_MEM_HOST) from_device(g, dist, dd, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *ranks, uint32_t mem,
+                      double *resid) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(ranks != nullptr, "null ranks");
+    need(iters >= 0, "iters must be >= 0");
+    need(dtype == PM_F32 || dtype == PM_F64, "dtype must be PM_F32 or PM_F64");
+    need(!g->has_self_loops,
+         "PageRank needs a graph without self loops (create it with PM_GRAPH_SKIP_SELF_LOOPS)");
+    const size_t es = dtype == PM_F64 ? 8 : 4;
+    const size_t bytes = (size_t)g->n * es;
+    void *dr = mem == PM_MEM_DEVICE ? ranks : g->scratch_buf(kSlotOut0, bytes);
+    double *dres = resid ? (double *)g->scratch_buf(kSlotAux, (size_t)std::max(iters, 1) * 8) : nullptr;
+    if (dtype == PM_F64)
+      run_pagerank<double>(g, iters, damping, (double *)dr, dres);
+    else
+      run_pagerank<float>(g, iters, damping, (float *)dr, dres);
+    if (mem == PM_MEM_HOST) from_device(g, ranks, dr, bytes, mem);
+    if (resid && iters > 0) from_device(g, resid, dres, (size_t)iters * 8, PM_MEM_HOST);
+    finish(g);
+  });
+}
+
+pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem, double *norm1) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(x0 != nullptr && y != nullptr, "null x0/y");
+    need(iters >= 0, "iters must be >= 0");
+    need(g->w_f32_out.p != nullptr, "graph has no float weights (pm_graph_set_weights_f32)");
+    const size_t bytes = (size_t)g->n * 4;
+    const float *dx = x0;
+    if (mem == PM_MEM_HOST) {
+      float *t = (float *)g->scratch_buf(kSlotIn0, bytes);
+      to_device(g, t, x0, bytes, mem);
+      dx = t;
+    }
+    float *dy = mem == PM_MEM_DEVICE ? y : (float *)g->scratch_buf(kSlotOut0, bytes);
+    double *dn = norm1 ? (double *)g->scratch_buf(kSlotAux, (size_t)std::max(iters, 1) * 8) : nullptr;
+    run_spmv(g, dx, iters, dy, dn);
+    if (mem == PM_MEM_HOST) from_device(g, y, dy, bytes, mem);
+    if (norm1 && iters > 0) from_device(g, norm1, dn, (size_t)iters * 8, PM_MEM_HOST);
+    finish(g);
+  });
+}
+
+pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
+                uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(prior != nullptr && psi != nullptr && log_prod != nullptr, "null prior/psi/log_prod");
+    need(iters >= 0, "iters must be >= 0");
+    need(mem == PM_MEM_HOST || (((uintptr_t)prior | (uintptr_t)log_prod) & 7) == 0,
+         "device prior/log_prod must be 8-byte aligned");
+    const size_t bytes = (size_t)g->n * 8;
+    float hpsi[4];
+    if (mem == PM_MEM_DEVICE) {
+      PM_CUDA(cudaMemcpy(hpsi, psi, sizeof hpsi, cudaMemcpyDeviceToHost));
+    } else {
+      memcpy(hpsi, psi, sizeof hpsi);
+    }
+    for (float p : hpsi) need(p > 0.0f && std::isfinite(p), "psi entries must be positive and finite");
+    const float *dp = prior;
+    if (mem == PM_MEM_HOST) {
+      float *t = (float *)g->scratch_buf(kSlotIn0, bytes);
+      to_device(g, t, prior, bytes, mem);
+      dp = t;
+    }
+    float *dout = mem == PM_MEM_DEVICE ? log_prod : (float *)g->scratch_buf(kSlotOut0, bytes);
+    run_bp(g, dp, hpsi, iters, dout);
+    if (mem == PM_MEM_HOST) from_device(g, log_prod, dout, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_timer_begin(pm_graph *g) {
+  return guard([&] {
+    enter(g);
+    PM_CUDA(cudaEventRecord(g->ev0, g->E.stream));
+  });
+}
+
+pm_status pm_timer_end(pm_graph *g, float *ms) {
+  return guard([&] {
+    enter(g);
+    PM_CUDA(cudaEventRecord(g->ev1, g->E.stream));
+    PM_CUDA(cudaEventSynchronize(g->ev1));
+    float t = 0.f;
+    PM_CUDA(cudaEventElapsedTime(&t, g->ev0, g->ev1));
+    if (ms) *ms = t;
+  });
+}
+
+pm_status pm_profile_enable(pm_graph *g, int enable) {
+  return guard([&] {
+    enter(g);
+    g->E.prof.enabled = enable != 0;
+  });
+}
+
+pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_t *passes,
+                          int reset) {
+  return guard([&] {
+    enter(g);
+    need(tag != nullptr, "null tag");
+    finish(g);
+    double tot = 0.0;
+    int64_t cnt = 0;
+    for (auto &r : g->E.prof.recs) {
+      if (r.tag != tag) continue;
+      float ms = 0.f;
+      PM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+      tot += ms;
+      ++cnt;
+    }
+    if (total_ms) *total_ms = tot;
+    if (passes) *passes = cnt;
+    if (reset) g->E.prof.clear();
+  });
+}
+
+pm_status pm_host_alloc(uint64_t bytes, void **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    PM_CUDA(cudaMallocHost(out, bytes ? bytes : 1));
+  });
+}
+
+pm_status pm_host_free(void *p) {
+  return guard([&] {
+    if (p) PM_CUDA(cudaFreeHost(p));
+  });
+}
+
+int64_t pm_kernel_launches(int reset) { return (int64_t)launches(reset != 0); }
+
+const char *pm_last_error(void) { return t_last_error.c_str(); }
+
+const char *pm_version(void) { return "polymer_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,428 @@
+// pm_graph.cu -- device graph construction: validation, self-loop removal,
+// CSC transpose, warp-group and heavy-chunk tables, the seeded R-MAT
+// generator and synthetic weights.  Off the hot path; sorts and scans use
+// CUB (library code) as plain primitives.
+#include <cub/cub.cuh>
+
+#include "pm_graph.cuh"
+
+namespace pm {
+
+static int grid1d(int64_t threads, int block = 256) {
+  int64_t b = (threads + block - 1) / block;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
+}
+
+#define GRID_STRIDE(i, count)                                                       \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (count);     \
+       i += (int64_t)gridDim.x * blockDim.x)
+
+// ---- validation -----------------------------------------------------------
+__global__ void k_validate(const int32_t *off, const int32_t *idx, int64_t n, int64_t m,
+                           unsigned int *err, unsigned int *self_loops) {
+  GRID_STRIDE(v, n) {
+    int32_t a = off[v], b = off[v + 1];
+    if (a > b || a < 0 || b > m) atomicOr(err, 1u);
+  }
+  GRID_STRIDE(e, m) {
+    int32_t d = idx[e];
+    if (d < 0 || d >= n) atomicOr(err, 2u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (off[0] != 0 || off[n] != m)) atomicOr(err, 4u);
+  (void)self_loops;
+}
+
+// Source row of CSR edge e (last r with off[r] <= e, skipping empty rows).
+__device__ __forceinline__ int32_t row_of(const int32_t *off, int64_t n, int64_t e) {
+  int64_t lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int64_t mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= e) lo = mid; else hi = mid - 1;
+  }
+  return (int32_t)lo;
+}
+
+__global__ void k_edge_src(const int32_t *off, int64_t n, int64_t m, int32_t *src) {
+  GRID_STRIDE(e, m) src[e] = row_of(off, n, e);
+}
+
+__global__ void k_self_flags(const int32_t *src, const int32_t *idx, int64_t m, int32_t *keep,
+                             unsigned int *count) {
+  unsigned int c = 0;
+  GRID_STRIDE(e, m) {
+    int32_t k = src[e] != idx[e];
+    keep[e] = k;
+    c += !k;
+  }
+  if (c) atomicAdd(count, c);
+}
+
+// new_off[r] = number of kept edges before old off[r]; pre has m+1 entries.
+__global__ void k_remap_offsets(const int32_t *off, const int32_t *pre, int64_t n, int32_t *noff) {
+  GRID_STRIDE(v, n + 1) noff[v] = pre[off[v]];
+}
+
+__global__ void k_compact_edges(const int32_t *idx, const int32_t *keep, const int32_t *pre,
+                                int64_t m, int32_t *nidx) {
+  GRID_STRIDE(e, m) if (keep[e]) nidx[pre[e]] = idx[e];
+}
+
+// ---- CSC ----------------------------------------------------------------
+__global__ void k_iota(int32_t *a, int64_t count) { GRID_STRIDE(i, count) a[i] = (int32_t)i; }
+
+__global__ void k_gather_src(const int32_t *src, const int32_t *eid, int64_t m, int32_t *tidx) {
+  GRID_STRIDE(p, m) tidx[p] = src[eid[p]];
+}
+
+// toff[v] = first position of key v in the sorted destination array.
+__global__ void k_lower_bound_offsets(const int32_t *keys, int64_t m, int64_t n, int32_t *toff) {
+  GRID_STRIDE(v, n + 1) {
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    toff[v] = (int32_t)lo;
+  }
+}
+
+// Symmetric graph: CSC slot p (row d, neighbour s) -> CSR edge s->d.
+__global__ void k_reverse_eid(const int32_t *off, const int32_t *idx, const int32_t *src,
+                              int64_t m, int32_t *eid) {
+  GRID_STRIDE(p, m) {
+    int32_t d = src[p], s = idx[p];
+    int64_t lo = off[s], hi = off[s + 1];
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (idx[mid] < d) lo = mid + 1; else hi = mid;
+    }
+    eid[p] = (int32_t)lo;
+  }
+}
+
+// ---- load-balance tables ---------------------------------------------------
+// gstart[g] = first row whose first edge is >= g*kGroupEdges, rounded down
+// to a multiple of 32; gstart[G] = n.
+__global__ void k_group_starts(const int32_t *off, int64_t n, int32_t G, int32_t *gstart) {
+  GRID_STRIDE(g, (int64_t)G + 1) {
+    if (g == G) { gstart[g] = (int32_t)n; continue; }
+    int64_t target = g * (int64_t)kGroupEdges;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (off[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    gstart[g] = (int32_t)(std::min<int64_t>(lo, n) & ~31ll);
+  }
+}
+
+__global__ void k_heavy_counts(const int32_t *off, int64_t n, int32_t *nch, int32_t *maxdeg) {
+  int32_t md = 0;
+  GRID_STRIDE(v, n) {
+    int32_t d = off[v + 1] - off[v];
+    nch[v] = d > kHeavyDeg ? (d + kChunkEdges - 1) / kChunkEdges : 0;
+    md = max(md, d);
+  }
+  atomicMax(maxdeg, md);
+}
+
+__global__ void k_heavy_rows(const int32_t *nch, const int32_t *first, int64_t n, int32_t *hrow) {
+  GRID_STRIDE(v, n) {
+    int32_t c = nch[v];
+    for (int32_t k = 0; k < c; ++k) hrow[first[v] + k] = (int32_t)v;
+  }
+}
+
+template <class T>
+__global__ void k_gather(const T *src, const int32_t *perm, int64_t count, T *dst) {
+  GRID_STRIDE(i, count) dst[i] = src[perm[i]];
+}
+
+// ---- R-MAT -----------------------------------------------------------------
+// Quadrant thresholds on a 24-bit draw: a = .57, a+b = .76, a+b+c = .95.
+constexpr uint32_t kRmatA = 9563013u, kRmatAB = 12750684u, kRmatABC = 15938355u;
+
+__global__ void k_rmat_keys(int scale, uint64_t seed, int64_t draws, int symmetric,
+                            uint64_t *keys) {
+  const uint64_t sentinel = (uint64_t)1 << (32 + scale);  // sorts after every edge
+  GRID_STRIDE(k, draws) {
+    uint32_t s = 0, d = 0;
+    for (int l = 0; l < scale; ++l) {
+      uint32_t u = (uint32_t)(hash64(seed, (uint64_t)k * (uint64_t)scale + (uint64_t)l) >> 40);
+      uint32_t row = u >= kRmatAB;
+      uint32_t col = (u >= kRmatA && u < kRmatAB) || u >= kRmatABC;
+      s = (s << 1) | row;
+      d = (d << 1) | col;
+    }
+    bool loop = s == d;
+    keys[k] = loop ? sentinel : (((uint64_t)s << 32) | d);
+    if (symmetric) keys[draws + k] = loop ? sentinel : (((uint64_t)d << 32) | s);
+  }
+}
+
+__global__ void k_keys_to_csr_idx(const uint64_t *keys, int64_t m, int32_t *idx) {
+  GRID_STRIDE(e, m) idx[e] = (int32_t)(keys[e] & 0xffffffffull);
+}
+
+__global__ void k_keys_offsets(const uint64_t *keys, int64_t m, int64_t n, int32_t *off) {
+  GRID_STRIDE(v, n + 1) {
+    uint64_t target = (uint64_t)v << 32;
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    off[v] = (int32_t)lo;
+  }
+}
+
+// Synthetic weights: the rules of the oracle (pmo_weight_int / _unit).
+__global__ void k_weights_i32(const int32_t *src, const int32_t *idx, int64_t m, uint64_t seed,
+                              int32_t wmax, int32_t *w) {
+  GRID_STRIDE(e, m) {
+    uint32_t u = (uint32_t)src[e], v = (uint32_t)idx[e];
+    uint32_t a = u < v ? u : v, b = u < v ? v : u;
+    w[e] = 1 + (int32_t)((hash64(seed, ((uint64_t)a << 32) | b) >> 32) % (uint64_t)wmax);
+  }
+}
+__global__ void k_weights_f32(const int32_t *src, const int32_t *idx, int64_t m, uint64_t seed,
+                              float *w) {
+  GRID_STRIDE(e, m) {
+    uint64_t key = ((uint64_t)(uint32_t)src[e] << 32) | (uint32_t)idx[e];
+    w[e] = (float)((hash64(seed, key) >> 40) + 1) * (1.0f / 16777216.0f);
+  }
+}
+__global__ void k_uniform_f32(uint64_t seed, int open, int64_t count, float *x) {
+  GRID_STRIDE(i, count) {
+    uint64_t h = hash64(seed, (uint64_t)i);
+    x[i] = open ? (float)(((h >> 41) << 1) | 1) * (1.0f / 16777216.0f)
+                : (float)(h >> 40) * (1.0f / 16777216.0f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
+  const int64_t n = g->n, m = g->m;
+  a.ngroups = (int32_t)((m + kGroupEdges - 1) / kGroupEdges);
+  if (a.ngroups < 1) a.ngroups = 1;
+  a.gstart.alloc((size_t)(a.ngroups + 1) * 4);
+  PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), n, a.ngroups,
+            a.gstart.as<int32_t>());
+  DevBuf nch((size_t)(n + 1) * 4), md(4);
+  PM_CUDA(cudaMemsetAsync(md.p, 0, 4, st));
+  PM_CUDA(cudaMemsetAsync(nch.p, 0, (size_t)(n + 1) * 4, st));
+  PM_LAUNCH(k_heavy_counts, grid1d(n), 256, 0, st, a.off.as<int32_t>(), n, nch.as<int32_t>(),
+            md.as<int32_t>());
+  a.hfirst.alloc((size_t)(n + 1) * 4);
+  size_t tmp = 0;
+  PM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, nch.as<int32_t>(), a.hfirst.as<int32_t>(),
+                                        (int)(n + 1), st));
+  DevBuf tb(tmp);
+  PM_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, nch.as<int32_t>(), a.hfirst.as<int32_t>(),
+                                        (int)(n + 1), st));
+  int32_t total = 0, maxdeg = 0;
+  PM_CUDA(cudaMemcpyAsync(&total, a.hfirst.as<int32_t>() + n, 4, cudaMemcpyDeviceToHost, st));
+  PM_CUDA(cudaMemcpyAsync(&maxdeg, md.p, 4, cudaMemcpyDeviceToHost, st));
+  PM_CUDA(cudaStreamSynchronize(st));
+  a.nchunks = total;
+  a.hrow.alloc((size_t)std::max(total, 1) * 4);
+  if (total > 0)
+    PM_LAUNCH(k_heavy_rows, grid1d(n), 256, 0, st, nch.as<int32_t>(), a.hfirst.as<int32_t>(), n,
+              a.hrow.as<int32_t>());
+  if (&a == &g->out) g->max_out_deg = maxdeg;
+}
+
+void finish_graph(pm_graph *g) {
+  cudaStream_t st = g->E.stream;
+  const int64_t n = g->n, m = g->m;
+  // Source of every CSR edge (needed for the transpose and weight rules).
+  DevBuf src((size_t)std::max<int64_t>(m, 1) * 4);
+  if (m) PM_LAUNCH(k_edge_src, grid1d(m), 256, 0, st, g->out.off.as<int32_t>(), n, m, src.as<int32_t>());
+  build_tables(g, g->out, st);
+  if (g->symmetric) {
+    g->in_eid.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+    if (m)
+      PM_LAUNCH(k_reverse_eid, grid1d(m), 256, 0, st, g->out.off.as<int32_t>(),
+                g->out.idx.as<int32_t>(), src.as<int32_t>(), m, g->in_eid.as<int32_t>());
+  } else {
+    // Stable radix sort of (dst, edge id): sources stay ascending per row.
+    int bits = 1;
+    while ((1ll << bits) < n) ++bits;
+    DevBuf kin((size_t)std::max<int64_t>(m, 1) * 4), kout((size_t)std::max<int64_t>(m, 1) * 4);
+    DevBuf vin((size_t)std::max<int64_t>(m, 1) * 4);
+    g->in_eid.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+    if (m) {
+      PM_CUDA(cudaMemcpyAsync(kin.p, g->out.idx.p, (size_t)m * 4, cudaMemcpyDeviceToDevice, st));
+      PM_LAUNCH(k_iota, grid1d(m), 256, 0, st, vin.as<int32_t>(), m);
+      size_t tmp = 0;
+      PM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin.as<int32_t>(), kout.as<int32_t>(),
+                                              vin.as<int32_t>(), g->in_eid.as<int32_t>(), (int)m, 0,
+                                              bits, st));
+      DevBuf tb(tmp);
+      PM_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, kin.as<int32_t>(), kout.as<int32_t>(),
+                                              vin.as<int32_t>(), g->in_eid.as<int32_t>(), (int)m, 0,
+                                              bits, st));
+    }
+    g->in.off.alloc((size_t)(n + 1) * 4);
+    g->in.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+    PM_LAUNCH(k_lower_bound_offsets, grid1d(n + 1), 256, 0, st, kout.as<int32_t>(), m, n,
+              g->in.off.as<int32_t>());
+    if (m)
+      PM_LAUNCH(k_gather_src, grid1d(m), 256, 0, st, src.as<int32_t>(), g->in_eid.as<int32_t>(), m,
+                g->in.idx.as<int32_t>());
+    build_tables(g, g->in, st);
+  }
+  // Views and workspaces.
+  GraphView &v = g->E.g;
+  v.n = (int32_t)n;
+  v.m = m;
+  v.out = g->out.view();
+  v.in = g->symmetric ? v.out : g->in.view();
+  const int64_t words = (n + 31) / 32 + 1;
+  g->bits0.alloc((size_t)words * 4);
+  g->bits1.alloc((size_t)words * 4);
+  g->queue0.alloc((size_t)(n + 1) * 4);
+  g->queue1.alloc((size_t)(n + 1) * 4);
+  g->defer.alloc((size_t)(n + 1) * 4);
+  g->partials.alloc((size_t)std::max(v.in.nchunks, 1) * 16);
+  g->cnt.alloc(3 * sizeof(Counters));
+  g->E.d_cnt = g->cnt.as<Counters>();
+  g->E.defer = g->defer.as<int32_t>();
+  g->E.partials = g->partials.p;
+  PM_CUDA(cudaStreamSynchronize(st));
+}
+
+void permute_weights_i32(pm_graph *g) {
+  const int64_t m = g->m;
+  g->w_i32_in.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+  if (m)
+    PM_LAUNCH(k_gather<int32_t>, grid1d(m), 256, 0, g->E.stream, g->w_i32_out.as<int32_t>(),
+              g->in_eid.as<int32_t>(), m, g->w_i32_in.as<int32_t>());
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+}
+void permute_weights_f32(pm_graph *g) {
+  const int64_t m = g->m;
+  g->w_f32_in.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+  if (m)
+    PM_LAUNCH(k_gather<float>, grid1d(m), 256, 0, g->E.stream, g->w_f32_out.as<float>(),
+              g->in_eid.as<int32_t>(), m, g->w_f32_in.as<float>());
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+}
+
+// Validate a CSR already on the device; optionally drop self loops.
+void ingest_csr(pm_graph *g, bool skip_self_loops) {
+  cudaStream_t st = g->E.stream;
+  const int64_t n = g->n, m = g->m;
+  DevBuf err(8);
+  PM_CUDA(cudaMemsetAsync(err.p, 0, 8, st));
+  PM_LAUNCH(k_validate, grid1d(std::max(n, m)), 256, 0, st, g->out.off.as<int32_t>(),
+            g->out.idx.as<int32_t>(), n, m, err.as<unsigned int>(), err.as<unsigned int>() + 1);
+  unsigned int h_err[2] = {0, 0};
+  PM_CUDA(cudaMemcpyAsync(h_err, err.p, 8, cudaMemcpyDeviceToHost, st));
+  PM_CUDA(cudaStreamSynchronize(st));
+  if (h_err[0])
+    fail(PM_ERR_BAD_GRAPH, std::string("invalid CSR:") + (h_err[0] & 1 ? " offsets not monotone" : "") +
+                               (h_err[0] & 2 ? " edge id out of range" : "") +
+                               (h_err[0] & 4 ? " offsets[0] != 0 or offsets[n] != m" : ""));
+  if (m == 0) return;
+  DevBuf src((size_t)m * 4), keep((size_t)m * 4), cntb(4);
+  PM_CUDA(cudaMemsetAsync(cntb.p, 0, 4, st));
+  PM_LAUNCH(k_edge_src, grid1d(m), 256, 0, st, g->out.off.as<int32_t>(), n, m, src.as<int32_t>());
+  PM_LAUNCH(k_self_flags, grid1d(m), 256, 0, st, src.as<int32_t>(), g->out.idx.as<int32_t>(), m,
+            keep.as<int32_t>(), cntb.as<unsigned int>());
+  unsigned int loops = 0;
+  PM_CUDA(cudaMemcpyAsync(&loops, cntb.p, 4, cudaMemcpyDeviceToHost, st));
+  PM_CUDA(cudaStreamSynchronize(st));
+  if (loops == 0) return;
+  if (!skip_self_loops) {
+    g->has_self_loops = true;
+    return;
+  }
+  DevBuf pre((size_t)(m + 1) * 4);
+  size_t tmp = 0;
+  PM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, keep.as<int32_t>(), pre.as<int32_t>(), (int)m, st));
+  DevBuf tb(tmp);
+  PM_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, keep.as<int32_t>(), pre.as<int32_t>(), (int)m, st));
+  int32_t m_new = (int32_t)(m - loops);
+  PM_CUDA(cudaMemcpyAsync(pre.as<int32_t>() + m, &m_new, 4, cudaMemcpyHostToDevice, st));
+  DevBuf noff((size_t)(n + 1) * 4), nidx((size_t)std::max<int32_t>(m_new, 1) * 4);
+  PM_LAUNCH(k_remap_offsets, grid1d(n + 1), 256, 0, st, g->out.off.as<int32_t>(), pre.as<int32_t>(), n,
+            noff.as<int32_t>());
+  PM_LAUNCH(k_compact_edges, grid1d(m), 256, 0, st, g->out.idx.as<int32_t>(), keep.as<int32_t>(),
+            pre.as<int32_t>(), m, nidx.as<int32_t>());
+  PM_CUDA(cudaStreamSynchronize(st));
+  g->out.off = std::move(noff);
+  g->out.idx = std::move(nidx);
+  g->m = m_new;
+}
+
+// Seeded R-MAT straight into the device CSR.
+void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed) {
+  cudaStream_t st = g->E.stream;
+  const int64_t n = (int64_t)1 << scale;
+  const int64_t draws = n * ef;
+  const int64_t nkeys = draws * (g->symmetric ? 2 : 1);
+  DevBuf a((size_t)nkeys * 8), b((size_t)nkeys * 8);
+  PM_LAUNCH(k_rmat_keys, grid1d(draws), 256, 0, st, scale, seed, draws, (int)g->symmetric,
+            a.as<uint64_t>());
+  cub::DoubleBuffer<uint64_t> db(a.as<uint64_t>(), b.as<uint64_t>());
+  size_t tmp = 0;
+  PM_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, db, (int)nkeys, 0, 33 + scale, st));
+  DevBuf tb(tmp);
+  PM_CUDA(cub::DeviceRadixSort::SortKeys(tb.p, tmp, db, (int)nkeys, 0, 33 + scale, st));
+  uint64_t *sorted = db.Current();
+  uint64_t *uniq = db.Alternate();
+  DevBuf nsel(8);
+  size_t tmp2 = 0;
+  PM_CUDA(cub::DeviceSelect::Unique(nullptr, tmp2, sorted, uniq, nsel.as<int64_t>(), (int64_t)nkeys, st));
+  DevBuf tb2(tmp2);
+  PM_CUDA(cub::DeviceSelect::Unique(tb2.p, tmp2, sorted, uniq, nsel.as<int64_t>(), (int64_t)nkeys, st));
+  int64_t nu = 0;
+  PM_CUDA(cudaMemcpyAsync(&nu, nsel.p, 8, cudaMemcpyDeviceToHost, st));
+  PM_CUDA(cudaStreamSynchronize(st));
+  // The sentinel (self loops) sorts last; drop it if present.
+  uint64_t last = 0;
+  PM_CUDA(cudaMemcpy(&last, uniq + (nu - 1), 8, cudaMemcpyDeviceToHost));
+  const int64_t m = (last >> 32) >= (uint64_t)n ? nu - 1 : nu;
+  if (m >= (1ll << 31) - 1) fail(PM_ERR_INVALID_ARG, "graph exceeds int32 edge offsets");
+  g->n = n;
+  g->m = m;
+  g->out.off.alloc((size_t)(n + 1) * 4);
+  g->out.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+  if (m) PM_LAUNCH(k_keys_to_csr_idx, grid1d(m), 256, 0, st, uniq, m, g->out.idx.as<int32_t>());
+  PM_LAUNCH(k_keys_offsets, grid1d(n + 1), 256, 0, st, uniq, m, n, g->out.off.as<int32_t>());
+  PM_CUDA(cudaStreamSynchronize(st));
+}
+
+void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float) {
+  cudaStream_t st = g->E.stream;
+  const int64_t n = g->n, m = g->m;
+  DevBuf src((size_t)std::max<int64_t>(m, 1) * 4);
+  if (m) PM_LAUNCH(k_edge_src, grid1d(m), 256, 0, st, g->out.off.as<int32_t>(), n, m, src.as<int32_t>());
+  if (is_float) {
+    g->w_f32_out.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+    if (m) PM_LAUNCH(k_weights_f32, grid1d(m), 256, 0, st, src.as<int32_t>(), g->out.idx.as<int32_t>(), m,
+                     seed, g->w_f32_out.as<float>());
+    permute_weights_f32(g);
+  } else {
+    g->w_i32_out.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+    if (m) PM_LAUNCH(k_weights_i32, grid1d(m), 256, 0, st, src.as<int32_t>(), g->out.idx.as<int32_t>(), m,
+                     seed, wmax, g->w_i32_out.as<int32_t>());
+    permute_weights_i32(g);
+  }
+}
+
+void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count) {
+  PM_LAUNCH(k_uniform_f32, grid1d(count), 256, 0, g->E.stream, seed, open, count, out);
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+}
+
+}  // namespace pm
+
+pm_graph::~pm_graph() {
+  if (E.stream) cudaStreamSynchronize(E.stream);
+  if (h_cnt) cudaFreeHost(h_cnt);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (E.stream) cudaStreamDestroy(E.stream);
+}

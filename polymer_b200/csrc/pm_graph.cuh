@@ -1,0 +1,103 @@
+// pm_graph.cuh -- the graph handle behind the C ABI.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "polymer.cuh"
+
+namespace pm {
+
+// Owning device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t b) { alloc(b); }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    reset();
+    p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0;
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void alloc(size_t b) {
+    reset();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+      fail(PM_ERR_OOM, "cudaMalloc of " + std::to_string(b) + " bytes failed: " +
+                           cudaGetErrorString(e));
+    }
+    bytes = b;
+  }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// One adjacency direction with its load-balance tables.
+struct AdjBuf {
+  DevBuf off, idx, gstart, hrow, hfirst;
+  int32_t ngroups = 0, nchunks = 0;
+  Adj view() const {
+    Adj a;
+    a.off = off.as<int32_t>();
+    a.idx = idx.as<int32_t>();
+    a.gstart = gstart.as<int32_t>();
+    a.hrow = hrow.as<int32_t>();
+    a.hfirst = hfirst.as<int32_t>();
+    a.ngroups = ngroups;
+    a.nchunks = nchunks;
+    return a;
+  }
+};
+
+}  // namespace pm
+
+struct pm_graph {
+  int device = 0;
+  int64_t n = 0, m = 0;
+  bool symmetric = false;
+  bool has_self_loops = false;
+  int32_t max_out_deg = 0;
+  pm::AdjBuf out, in;     // in.* empty when symmetric (views alias out)
+  pm::DevBuf in_eid;      // CSC slot -> CSR edge id (directed graphs)
+  pm::DevBuf w_i32_out, w_i32_in, w_f32_out, w_f32_in;
+  pm::Engine E;
+  pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, partials;
+  pm::Counters *h_cnt = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<pm::DevBuf> scratch;  // per-call workspaces kept across calls
+
+  pm::VertexSubset subset(int k) {
+    pm::VertexSubset s;
+    s.n = (int32_t)n;
+    s.bits = (k == 0 ? bits0 : bits1).as<uint32_t>();
+    s.queue = (k == 0 ? queue0 : queue1).as<int32_t>();
+    return s;
+  }
+  // Scratch slot i with at least bytes capacity (kept for reuse).
+  void *scratch_buf(size_t i, size_t bytes) {
+    if (scratch.size() <= i) scratch.resize(i + 1);
+    if (scratch[i].bytes < bytes) scratch[i].alloc(bytes);
+    return scratch[i].p;
+  }
+  ~pm_graph();
+};
+
+namespace pm {
+// Builds every derived structure (CSC, groups, heavy chunks, workspaces)
+// once out.off / out.idx hold a validated CSR on the device.
+void finish_graph(pm_graph *g);
+// Writes in_w = out_w[in_eid] (or aliases for symmetric graphs).
+void permute_weights_i32(pm_graph *g);
+void permute_weights_f32(pm_graph *g);
+}  // namespace pm

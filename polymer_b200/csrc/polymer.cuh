@@ -1,0 +1,788 @@
+// polymer.cuh -- the B200 edgeMap / vertexMap engine.
+//
+// This header keeps the programming model of Polymer's polymer.h: a graph,
+// a vertexSubset (frontier), edgeMap(G, frontier, F, threshold, option),
+// vertexMap and vertexFilter, with user functors that expose
+//   cond(d)                 -> should d still be updated       (polymer.h:2240-2309)
+//   updateAtomic(s, d, w)   -> apply s->d, true if d activated (sparse / dense push)
+// and, for the reducing dense pull (edgeMapDenseReduce, polymer.h:1097-1168),
+//   identity()/edge(s,d,w)/combine(a,b)/commit(d,acc)  (initFunc/reduceFunc/
+//   combineFunc of the reference; commit also runs the fused vertexMap).
+// Functors are __device__ objects passed by value to the kernels and inlined
+// at compile time, as the reference's templates are inlined on the CPU.
+//
+// Device layout (one GPU, everything resident in HBM):
+//   CSR out-edges and CSC in-edges, int32 offsets (n+1) and ids (m);
+//   a frontier is a bitmap of ceil(n/32) words plus, when it came from a
+//   sparse round, a queue of int32 ids (the reference's LocalFrontier b / s,
+//   polymer.h:527-639).
+// Kernels:
+//   k_sparse_push   queue -> queue+bitmap, CTA / warp / scan-gather expansion,
+//                   warp-aggregated queue appends          (edgeMapSparseV3)
+//   k_dense_pull    bitmap -> bitmap, one thread per vertex over the CSC with
+//                   early exit on cond, long rows deferred to one warp each
+//                                                          (edgeMapDense*)
+//   k_pull_reduce   bitmap -> bitmap, edge-balanced warp groups with a
+//                   segmented warp reduction; rows above kHeavyDeg are summed
+//                   by k_heavy_reduce chunks first          (edgeMapDenseReduce)
+//   k_dense_push    bitmap -> bitmap over the CSR with atomics
+//                                                          (edgeMapDenseForward)
+#pragma once
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "pm_common.cuh"
+
+namespace pm {
+
+constexpr int kGroupEdges = 1024;  // edge window that defines one warp group
+constexpr int kHeavyDeg = 1024;    // rows above this degree are split in chunks
+constexpr int kChunkEdges = 2048;  // edges of one heavy chunk (one CTA)
+constexpr int kChunkThreads = 256;
+constexpr int kPullScan = 32;      // edges a thread scans before deferring a row
+constexpr int kCtaExpand = 512;    // sparse push: CTA-wide expansion above this degree
+
+// One adjacency direction.
+struct Adj {
+  const int32_t *off = nullptr;     // n+1
+  const int32_t *idx = nullptr;     // m
+  const int32_t *gstart = nullptr;  // ngroups+1 warp-group row starts (32-aligned; last = n)
+  const int32_t *hrow = nullptr;    // heavy chunk -> row
+  const int32_t *hfirst = nullptr;  // row -> its first heavy chunk (rows with deg > kHeavyDeg)
+  int32_t ngroups = 0;
+  int32_t nchunks = 0;
+};
+
+struct GraphView {
+  int32_t n = 0;
+  int64_t m = 0;
+  Adj out;  // CSR
+  Adj in;   // CSC (aliases out for symmetric graphs)
+};
+
+__device__ __forceinline__ bool test_bit(const uint32_t *__restrict__ b, int v) {
+  return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
+}
+// Sets bit v; true if this call set it (the bit was clear).
+__device__ __forceinline__ bool set_bit_new(uint32_t *b, int v) {
+  uint32_t mask = 1u << (v & 31);
+  return !(atomicOr(b + (v >> 5), mask) & mask);
+}
+
+template <class W>
+__device__ __forceinline__ W load_w(const W *w, int64_t e) {
+  return w ? __ldg(w + e) : W(0);
+}
+
+// ---------------------------------------------------------------------------
+// Warp-collective append of activated vertices to the next queue.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void emit_queue(bool act, int d, int32_t *queue, int32_t qcap,
+                                           Counters *cnt) {
+  unsigned bal = __ballot_sync(0xffffffffu, act);
+  if (!bal) return;
+  int lane = lane_id();
+  int leader = __ffs(bal) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(&cnt->size, (unsigned long long)__popc(bal));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (act) {
+    unsigned long long p = base + __popc(bal & ((1u << lane) - 1u));
+    if (p < (unsigned long long)qcap)
+      queue[p] = d;
+    else
+      atomicOr(&cnt->err, (unsigned)kErrQueueOverflow);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse push (edgeMapSparseV3, polymer.h:1928-2003): expand the out-edges of
+// every queued vertex; d joins the next frontier when cond(d) &&
+// updateAtomic(s, d, w) holds and its bit was not yet set this round.
+// Load balance: rows >= kCtaExpand are expanded by the whole CTA, rows >= 32
+// by one warp, the rest through a CTA-wide scan of their degrees.
+// ---------------------------------------------------------------------------
+template <class F, class W>
+__device__ __forceinline__ bool push_edge(const GraphView &g, F &f, const W *w, int s, int64_t e,
+                                          uint32_t *next_bits, int &d_out) {
+  int d = __ldg(g.out.idx + e);
+  d_out = d;
+  if (f.cond(d) && f.updateAtomic(s, d, load_w(w, e))) return set_bit_new(next_bits, d);
+  return false;
+}
+
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t *__restrict__ queue,
+                                                     int32_t qsize, F f, const W *__restrict__ w,
+                                                     int32_t *__restrict__ next_queue,
+                                                     uint32_t *__restrict__ next_bits, int32_t qcap,
+                                                     Counters *cnt) {
+  __shared__ int s_pos[256];
+  __shared__ int s_v[256];
+  __shared__ int s_o[256];
+  __shared__ int s_warp_tot[8];
+  __shared__ int s_owner, s_cv, s_co, s_cd;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  unsigned long long my_edges = 0;
+  for (int64_t base = (int64_t)blockIdx.x * 256; base < qsize; base += (int64_t)gridDim.x * 256) {
+    int64_t i = base + tid;
+    int v = -1, o = 0, deg = 0;
+    if (i < qsize) {
+      v = queue[i];
+      o = __ldg(g.out.off + v);
+      deg = __ldg(g.out.off + v + 1) - o;
+    }
+    // CTA-wide expansion of long rows.
+    for (;;) {
+      if (tid == 0) s_owner = -1;
+      __syncthreads();
+      if (deg >= kCtaExpand) s_owner = tid;
+      __syncthreads();
+      int owner = s_owner;
+      if (owner < 0) break;
+      if (tid == owner) { s_cv = v; s_co = o; s_cd = deg; deg = 0; }
+      __syncthreads();
+      int cv = s_cv, co = s_co, cd = s_cd;
+      for (int r = 0; r < cd; r += 256) {
+        int k = r + tid, d = -1;
+        bool act = k < cd && push_edge(g, f, w, cv, (int64_t)co + k, next_bits, d);
+        if (act) my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+        emit_queue(act, d, next_queue, qcap, cnt);
+      }
+      __syncthreads();
+    }
+    // Warp-wide expansion of medium rows.
+    for (;;) {
+      unsigned bal = __ballot_sync(0xffffffffu, deg >= 32);
+      if (!bal) break;
+      int leader = __ffs(bal) - 1;
+      int wv = __shfl_sync(0xffffffffu, v, leader);
+      int wo = __shfl_sync(0xffffffffu, o, leader);
+      int wd = __shfl_sync(0xffffffffu, deg, leader);
+      if (lane == leader) deg = 0;
+      for (int r = 0; r < wd; r += 32) {
+        int k = r + lane, d = -1;
+        bool act = k < wd && push_edge(g, f, w, wv, (int64_t)wo + k, next_bits, d);
+        if (act) my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+        emit_queue(act, d, next_queue, qcap, cnt);
+      }
+    }
+    // Scan-based gather of the short rows.
+    int wtot;
+    int pos = warp_excl_scan(deg, &wtot);
+    if (lane == 0) s_warp_tot[wid] = wtot;
+    __syncthreads();
+    int woff = 0, total = 0;
+    for (int k = 0; k < 8; ++k) {
+      if (k < wid) woff += s_warp_tot[k];
+      total += s_warp_tot[k];
+    }
+    s_pos[tid] = pos + woff;
+    s_v[tid] = v;
+    s_o[tid] = o;
+    __syncthreads();
+    for (int r = 0; r < total; r += 256) {
+      int k = r + tid, d = -1;
+      bool act = false;
+      if (k < total) {
+        int lo = 0, hi = 255;  // last j with s_pos[j] <= k
+        while (lo < hi) {
+          int mid = (lo + hi + 1) >> 1;
+          if (s_pos[mid] <= k) lo = mid; else hi = mid - 1;
+        }
+        act = push_edge(g, f, w, s_v[lo], (int64_t)s_o[lo] + (k - s_pos[lo]), next_bits, d);
+      }
+      if (act) my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+      emit_queue(act, d, next_queue, qcap, cnt);
+    }
+    __syncthreads();
+  }
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_edges) atomicAdd(&cnt->edges, my_edges);
+}
+
+// ---------------------------------------------------------------------------
+// Dense pull with early exit (edgeMapDenseDynamic polymer.h:1170-1261,
+// edgeMapDenseNoRep numa-BFS.C:113-159): for every vertex v with cond(v),
+// scan in-neighbours s in the frontier, call updateAtomic(s, v, w) and stop
+// once cond(v) is false.  One thread per vertex scans up to kPullScan edges;
+// rows still open after that are deferred to k_dense_pull_defer (one warp
+// per row).  A warp owns 32 consecutive vertices = one bitmap word.
+// ---------------------------------------------------------------------------
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_dense_pull(GraphView g, const uint32_t *__restrict__ cur,
+                                                    F f, const W *__restrict__ w,
+                                                    uint32_t *__restrict__ next,
+                                                    int32_t *__restrict__ defer, Counters *cnt,
+                                                    Counters *dcnt) {
+  const int lane = lane_id();
+  unsigned long long my_edges = 0, my_size = 0;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const int64_t ntot = ((int64_t)g.n + 31) & ~31ll;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += nthreads) {
+    int v = (int)t;
+    bool act = false, deferred = false;
+    if (v < g.n && f.cond(v)) {
+      int o0 = __ldg(g.in.off + v), o1 = __ldg(g.in.off + v + 1);
+      int lim = min(o1, o0 + kPullScan);
+      int e = o0;
+      for (; e < lim; ++e) {
+        int s = __ldg(g.in.idx + e);
+        if (test_bit(cur, s) && f.updateAtomic(s, v, load_w(w, e))) act = true;
+        if (!f.cond(v)) break;
+      }
+      deferred = (e == lim) && lim < o1 && f.cond(v);
+    }
+    unsigned word = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) next[v >> 5] = word;
+    if (act) {
+      my_size++;
+      my_edges += __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+    }
+    unsigned db = __ballot_sync(0xffffffffu, deferred);
+    if (db) {
+      int leader = __ffs(db) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&dcnt->size, (unsigned long long)__popc(db));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (deferred) defer[base + __popc(db & ((1u << lane) - 1u))] = v;
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_size) {
+    atomicAdd(&cnt->size, my_size);
+    atomicAdd(&cnt->edges, my_edges);
+  }
+}
+
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
+                                                          const uint32_t *__restrict__ cur, F f,
+                                                          const W *__restrict__ w,
+                                                          uint32_t *__restrict__ next,
+                                                          const int32_t *__restrict__ defer,
+                                                          Counters *cnt, const Counters *dcnt) {
+  const int lane = lane_id();
+  const int64_t nd = (int64_t)dcnt->size;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t k = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < nd; k += nwarps) {
+    int v = defer[k];
+    int o0 = __ldg(g.in.off + v) + kPullScan, o1 = __ldg(g.in.off + v + 1);
+    bool act = false, open = true;
+    for (int base = o0; base < o1 && open; base += 32) {
+      int e = base + lane;
+      int s = e < o1 ? __ldg(g.in.idx + e) : 0;
+      unsigned bal = __ballot_sync(0xffffffffu, e < o1 && test_bit(cur, s));
+      while (bal && open) {
+        int l = __ffs(bal) - 1;
+        bal &= bal - 1;
+        int ss = __shfl_sync(0xffffffffu, s, l);
+        int ok = 0, c = 1;
+        if (lane == 0) {
+          ok = f.updateAtomic(ss, v, load_w(w, (int64_t)base + l));
+          c = f.cond(v);
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        act |= ok != 0;
+        open = c != 0;
+      }
+    }
+    // The first kernel may already have set v's bit (and counted it).
+    if (act && lane == 0 && set_bit_new(next, v)) {
+      atomicAdd(&cnt->size, 1ull);
+      atomicAdd(&cnt->edges, (unsigned long long)(__ldg(g.out.off + v + 1) - __ldg(g.out.off + v)));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense pull-reduce (edgeMapDenseReduce, polymer.h:1097-1168).  A warp takes
+// one group: the 32-aligned rows whose first in-edge falls in a window of
+// kGroupEdges edges.  It walks them 32 rows at a time, lays their edges out
+// flat (consecutive rows are consecutive in the CSC, so loads coalesce),
+// evaluates f.edge() per edge, folds each row with a segmented warp
+// reduction into shared memory and lets the row's lane run f.commit() (the
+// fused vertexMap).  Rows with more than kHeavyDeg edges are reduced first
+// by k_heavy_reduce (one CTA per kChunkEdges chunk) into partials[], which
+// the owning lane folds in chunk order -- every result is deterministic.
+// ---------------------------------------------------------------------------
+template <class F, class W>
+__global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f,
+                                                                const W *__restrict__ w,
+                                                                typename F::Acc *partials) {
+  using Acc = typename F::Acc;
+  __shared__ Acc s_red[kChunkThreads / 32];
+  const int c = blockIdx.x;
+  if (c >= g.in.nchunks) return;
+  const int r = __ldg(g.in.hrow + c);
+  const int k = c - __ldg(g.in.hfirst + r);
+  const int64_t e0 = (int64_t)__ldg(g.in.off + r) + (int64_t)k * kChunkEdges;
+  const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.in.off + r + 1));
+  Acc acc = f.identity();
+  if (f.cond(r)) {
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads)
+      acc = f.combine(acc, f.edge(__ldg(g.in.idx + e), r, load_w(w, e)));
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) acc = f.combine(acc, shfl_down(acc, d));
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Acc t = s_red[0];
+    for (int i = 1; i < kChunkThreads / 32; ++i) t = f.combine(t, s_red[i]);
+    partials[c] = t;
+  }
+}
+
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
+                                                     const typename F::Acc *__restrict__ partials,
+                                                     uint32_t *__restrict__ next, Counters *cnt) {
+  using Acc = typename F::Acc;
+  __shared__ Acc s_acc[8][32];
+  const int lane = lane_id(), wid = threadIdx.x >> 5;
+  const int grp = blockIdx.x * 8 + wid;
+  if (grp >= g.in.ngroups) return;
+  const int r_begin = __ldg(g.in.gstart + grp), r_end = __ldg(g.in.gstart + grp + 1);
+  unsigned long long my_size = 0, my_edges = 0;
+  double my_aux = 0.0;
+  for (int rb = r_begin; rb < r_end; rb += 32) {
+    const int r = rb + lane;
+    const bool valid = r < r_end;
+    int o0 = 0, deg = 0;
+    bool live = false;
+    if (valid) {
+      o0 = __ldg(g.in.off + r);
+      deg = __ldg(g.in.off + r + 1) - o0;
+      live = f.cond(r);
+    }
+    const bool heavy = deg > kHeavyDeg;
+    const int ldeg = (live && !heavy) ? deg : 0;
+    int total;
+    const int pos = warp_excl_scan(ldeg, &total);
+    s_acc[wid][lane] = f.identity();
+    __syncwarp();
+    for (int c = 0; c < total; c += 32) {
+      const int q = c + lane;
+      const bool active = q < total;
+      // owner lane j: the last lane whose flat start is <= q
+      int j = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        int cand = j + step;
+        int pc = __shfl_sync(0xffffffffu, pos, cand);
+        if (pc <= q) j = cand;
+      }
+      const int oj = __shfl_sync(0xffffffffu, o0, j);
+      const int pj = __shfl_sync(0xffffffffu, pos, j);
+      Acc v = f.identity();
+      if (active) {
+        const int64_t e = (int64_t)oj + (q - pj);
+        v = f.edge(__ldg(g.in.idx + e), rb + j, load_w(w, e));
+      }
+      const int key = active ? j : 32 + lane;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        Acc t = shfl_down(v, d);
+        int tk = __shfl_down_sync(0xffffffffu, key, d);
+        if (lane + d < 32 && tk == key) v = f.combine(v, t);
+      }
+      const int prev_key = __shfl_up_sync(0xffffffffu, key, 1);
+      if (active && (lane == 0 || prev_key != key)) s_acc[wid][j] = f.combine(s_acc[wid][j], v);
+      __syncwarp();
+    }
+    Acc acc = s_acc[wid][lane];
+    if (live && heavy) {
+      const int first = __ldg(g.in.hfirst + r);
+      const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
+      for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);
+    }
+    const bool act = live && f.commit(r, acc, my_aux);
+    const unsigned word = __ballot_sync(0xffffffffu, act);
+    if (next && lane == 0) next[rb >> 5] = word;
+    if (act) {
+      my_size++;
+      my_edges += __ldg(g.out.off + r + 1) - __ldg(g.out.off + r);
+    }
+    __syncwarp();
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  my_aux = warp_sum(my_aux);
+  if (lane == 0) {
+    if (my_size) {
+      atomicAdd(&cnt->size, my_size);
+      atomicAdd(&cnt->edges, my_edges);
+    }
+    if (my_aux != 0.0) atomicAdd(&cnt->daux, my_aux);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense push (edgeMapDenseForward, polymer.h:970-1032): every vertex in the
+// frontier bitmap pushes over its out-edges with atomics; d's bit is set
+// when cond(d) && updateAtomic(s, d, w).  Same warp groups as the pull, over
+// the CSR, with inactive rows contributing no edges; heavy rows are pushed
+// by the chunk kernel.
+// ---------------------------------------------------------------------------
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_dense_push(GraphView g, const uint32_t *__restrict__ cur,
+                                                    F f, const W *__restrict__ w,
+                                                    uint32_t *__restrict__ next, Counters *cnt) {
+  const int lane = lane_id(), wid = threadIdx.x >> 5;
+  const int grp = blockIdx.x * 8 + wid;
+  if (grp >= g.out.ngroups) return;
+  const int r_begin = __ldg(g.out.gstart + grp), r_end = __ldg(g.out.gstart + grp + 1);
+  unsigned long long my_size = 0, my_edges = 0;
+  for (int rb = r_begin; rb < r_end; rb += 32) {
+    const int r = rb + lane;
+    int o0 = 0, deg = 0;
+    if (r < r_end && test_bit(cur, r)) {
+      o0 = __ldg(g.out.off + r);
+      deg = __ldg(g.out.off + r + 1) - o0;
+    }
+    const int ldeg = deg > kHeavyDeg ? 0 : deg;
+    int total;
+    const int pos = warp_excl_scan(ldeg, &total);
+    for (int c = 0; c < total; c += 32) {
+      const int q = c + lane;
+      int j = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        int cand = j + step;
+        if (__shfl_sync(0xffffffffu, pos, cand) <= q) j = cand;
+      }
+      const int oj = __shfl_sync(0xffffffffu, o0, j);
+      const int pj = __shfl_sync(0xffffffffu, pos, j);
+      if (q < total) {
+        const int64_t e = (int64_t)oj + (q - pj);
+        const int d = __ldg(g.out.idx + e);
+        if (f.cond(d) && f.updateAtomic(rb + j, d, load_w(w, e)) && set_bit_new(next, d)) {
+          my_size++;
+          my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+        }
+      }
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_size) {
+    atomicAdd(&cnt->size, my_size);
+    atomicAdd(&cnt->edges, my_edges);
+  }
+}
+
+template <class F, class W>
+__global__ void __launch_bounds__(kChunkThreads) k_heavy_push(GraphView g,
+                                                              const uint32_t *__restrict__ cur, F f,
+                                                              const W *__restrict__ w,
+                                                              uint32_t *__restrict__ next,
+                                                              Counters *cnt) {
+  const int c = blockIdx.x;
+  if (c >= g.out.nchunks) return;
+  const int r = __ldg(g.out.hrow + c);
+  if (!test_bit(cur, r)) return;
+  const int k = c - __ldg(g.out.hfirst + r);
+  const int64_t e0 = (int64_t)__ldg(g.out.off + r) + (int64_t)k * kChunkEdges;
+  const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.out.off + r + 1));
+  unsigned long long my_size = 0, my_edges = 0;
+  for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads) {
+    const int d = __ldg(g.out.idx + e);
+    if (f.cond(d) && f.updateAtomic(r, d, load_w(w, e)) && set_bit_new(next, d)) {
+      my_size++;
+      my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  if (lane_id() == 0 && my_size) {
+    atomicAdd(&cnt->size, my_size);
+    atomicAdd(&cnt->edges, my_edges);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Frontier plumbing.
+// ---------------------------------------------------------------------------
+// Bitmap -> queue (LocalFrontier::toSparse, polymer.h:552-567): ballot/popc
+// compaction, one queue atomic per warp; also counts |F| and sum outdeg(F).
+__global__ void k_bits_to_queue(int32_t n, const int32_t *__restrict__ out_off,
+                                const uint32_t *__restrict__ bits, int32_t *__restrict__ queue,
+                                Counters *cnt);
+// Queue -> bitmap (LocalFrontier::toDense, polymer.h:594-601).
+__global__ void k_queue_to_bits(const int32_t *__restrict__ queue, int32_t size,
+                                uint32_t *__restrict__ bits);
+// |F| and sum outdeg(F) of a bitmap (vertexCounter, polymer.h:2311-2338).
+__global__ void k_bits_stats(int32_t n, const int32_t *__restrict__ out_off,
+                             const uint32_t *__restrict__ bits, Counters *cnt);
+
+// vertexMap over a bitmap (polymer.h:2340-2381).
+template <class F>
+__global__ void k_vertex_map_bits(int32_t n, const uint32_t *__restrict__ bits, F f) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+    if (test_bit(bits, (int)v)) f((int)v);
+}
+// vertexMap over all vertices.
+template <class F>
+__global__ void k_vertex_map_all(int32_t n, F f) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) f((int)v);
+}
+// vertexFilter (polymer.h:2399-2441): out bit = in bit && f(v); counts |out|.
+template <class F>
+__global__ void k_vertex_filter(int32_t n, const int32_t *__restrict__ out_off,
+                                const uint32_t *__restrict__ bits, F f,
+                                uint32_t *__restrict__ out, Counters *cnt) {
+  const int lane = lane_id();
+  const int64_t ntot = ((int64_t)n + 31) & ~31ll;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long my_size = 0, my_edges = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += stride) {
+    int v = (int)t;
+    bool keep = v < n && test_bit(bits, v) && f(v);
+    unsigned word = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) out[v >> 5] = word;
+    if (keep) {
+      my_size++;
+      my_edges += __ldg(out_off + v + 1) - __ldg(out_off + v);
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_size) {
+    atomicAdd(&cnt->size, my_size);
+    atomicAdd(&cnt->edges, my_edges);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+enum Option { DENSE = 0, DENSE_PARALLEL = 1, DENSE_FORWARD = 2 };  // polymer.h:913-915
+
+// A frontier on the device (the reference's vertices / LocalFrontier).
+struct VertexSubset {
+  int32_t n = 0;
+  uint32_t *bits = nullptr;   // ceil(n/32) words, always valid
+  int32_t *queue = nullptr;   // capacity n; valid when has_queue
+  bool has_queue = false;
+  int64_t size = 0;           // |F|
+  int64_t edges = 0;          // sum of out-degrees of F
+  int64_t words() const { return ((int64_t)n + 31) / 32; }
+};
+
+// CUDA-event brackets around application passes (pm_profile_*).
+struct Profiler {
+  struct Rec {
+    std::string tag;
+    cudaEvent_t a, b;
+  };
+  bool enabled = false;
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t take() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    PM_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+  void begin(const char *tag, cudaStream_t s) {
+    if (!enabled) return;
+    Rec r{tag, take(), take()};
+    PM_CUDA(cudaEventRecord(r.a, s));
+    recs.push_back(r);
+  }
+  void end(cudaStream_t s) {
+    if (!enabled || recs.empty()) return;
+    PM_CUDA(cudaEventRecord(recs.back().b, s));
+  }
+  void clear() {
+    for (auto &r : recs) {
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    recs.clear();
+  }
+  ~Profiler() {
+    clear();
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+// Per-graph execution context: stream, counters, scratch.
+struct Engine {
+  GraphView g;
+  cudaStream_t stream = nullptr;
+  Counters *d_cnt = nullptr;   // [0] next frontier, [1] deferred rows, [2] aux
+  Counters *h_cnt = nullptr;   // pinned mirror
+  int32_t *defer = nullptr;    // n
+  void *partials = nullptr;    // max(in.nchunks, 1) * 16 bytes
+  int num_sms = 148;
+  Profiler prof;
+  const char *tag = "edgemap";  // profile tag of the running application
+
+  int grid_for(int64_t threads, int block = 256, int per_sm = 8) const {
+    int64_t b = (threads + block - 1) / block;
+    int64_t cap = (int64_t)num_sms * per_sm;
+    return (int)std::max<int64_t>(1, std::min(b, cap));
+  }
+  void reset_counters() {
+    PM_CUDA(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(Counters), stream));
+  }
+  // Blocks until the counters are on the host.
+  const Counters *read_counters() {
+    PM_CUDA(cudaMemcpyAsync(h_cnt, d_cnt, 3 * sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    for (int i = 0; i < 3; ++i)
+      if (h_cnt[i].err) {
+        unsigned e = h_cnt[i].err;
+        fail(e & kErrTimeout ? PM_ERR_TIMEOUT : PM_ERR_CUDA,
+             std::string("device error word ") + std::to_string(e) +
+                 (e & kErrQueueOverflow ? " (queue overflow)" : "") +
+                 (e & kErrRange ? " (id out of range)" : ""));
+      }
+    return h_cnt;
+  }
+};
+
+// Recount s.size / s.edges from s.bits (vertexCounter, polymer.h:2311-2338).
+void subset_recount(Engine &E, VertexSubset &s);
+// Make sure s.queue holds s (compaction of the bitmap).
+void subset_to_queue(Engine &E, VertexSubset &s);
+// Single vertex frontier.
+void subset_single(Engine &E, VertexSubset &s, int32_t v);
+// All vertices.
+void subset_all(Engine &E, VertexSubset &s);
+void subset_clear(Engine &E, VertexSubset &s);
+
+// Direction switch of edgeMap (polymer.h:2247, 2260): dense when
+// |F| + outdeg(F) >= threshold.
+inline bool go_dense(const VertexSubset &cur, int64_t threshold) {
+  return cur.size + cur.edges >= threshold;
+}
+
+template <class W, class F>
+void launch_sparse_push(Engine &E, VertexSubset &cur, F f, const W *w_out, VertexSubset &next) {
+  subset_to_queue(E, cur);
+  PM_CUDA(cudaMemsetAsync(next.bits, 0, next.words() * 4, E.stream));
+  if (cur.size > 0) {
+    int grid = E.grid_for(cur.size, 256, 8);
+    PM_LAUNCH((k_sparse_push<F, W>), grid, 256, 0, E.stream, E.g, cur.queue, (int32_t)cur.size, f,
+              w_out, next.queue, next.bits, next.n, E.d_cnt);
+  }
+  next.has_queue = true;
+}
+
+template <class W, class F>
+void launch_dense_pull(Engine &E, VertexSubset &cur, F f, const W *w_in, VertexSubset &next) {
+  int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
+  PM_LAUNCH((k_dense_pull<F, W>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, E.g, cur.bits, f,
+            w_in, next.bits, E.defer, E.d_cnt, E.d_cnt + 1);
+  PM_LAUNCH((k_dense_pull_defer<F, W>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.bits, f, w_in,
+            next.bits, E.defer, E.d_cnt, E.d_cnt + 1);
+  next.has_queue = false;
+}
+
+template <class W, class F>
+void launch_dense_push(Engine &E, VertexSubset &cur, F f, const W *w_out, VertexSubset &next) {
+  PM_CUDA(cudaMemsetAsync(next.bits, 0, next.words() * 4, E.stream));
+  if (E.g.out.nchunks > 0)
+    PM_LAUNCH((k_heavy_push<F, W>), E.g.out.nchunks, kChunkThreads, 0, E.stream, E.g, cur.bits, f,
+              w_out, next.bits, E.d_cnt);
+  PM_LAUNCH((k_dense_push<F, W>), (E.g.out.ngroups + 7) / 8, 256, 0, E.stream, E.g, cur.bits, f,
+            w_out, next.bits, E.d_cnt);
+  next.has_queue = false;
+}
+
+// Pull-reduce over the CSC into counters cnt (size / edges of the output,
+// daux = sum of the FP64 values commit() adds); next_bits may be null.
+template <class W, class F>
+void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Counters *cnt) {
+  static_assert(sizeof(typename F::Acc) <= 16, "accumulator larger than the partials slot");
+  using Acc = typename F::Acc;
+  Acc *partials = reinterpret_cast<Acc *>(E.partials);
+  if (E.g.in.nchunks > 0)
+    PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in,
+              partials);
+  PM_LAUNCH((k_pull_reduce<F, W>), (E.g.in.ngroups + 7) / 8, 256, 0, E.stream, E.g, f, w_in,
+            (const Acc *)partials, next_bits, cnt);
+}
+
+// edgeMap (polymer.h:2240-2309): sparse push below the threshold, otherwise
+// dense pull (option DENSE / DENSE_PARALLEL) or dense push (DENSE_FORWARD).
+// On return next holds the output frontier with its size and out-degree sum.
+template <class W = int, class F>
+void edgeMap(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_t threshold,
+             Option option = DENSE, const W *w_out = nullptr, const W *w_in = nullptr,
+             bool *took_dense = nullptr) {
+  E.reset_counters();
+  const bool dense = go_dense(cur, threshold);
+  if (took_dense) *took_dense = dense;
+  E.prof.begin(E.tag, E.stream);
+  if (dense) {
+    if (option == DENSE_FORWARD)
+      launch_dense_push<W>(E, cur, f, w_out, next);
+    else
+      launch_dense_pull<W>(E, cur, f, w_in, next);
+  } else {
+    launch_sparse_push<W>(E, cur, f, w_out, next);
+  }
+  E.prof.end(E.stream);
+  const Counters *h = E.read_counters();
+  next.size = (int64_t)h[0].size;
+  next.edges = (int64_t)h[0].edges;
+}
+
+// edgeMap with a reducing dense path (edgeMapCustom numa-Components.C:121-175
+// / edgeMapDenseReduce): dense rounds run the pull-reduce with fused commit,
+// sparse rounds the push with updateAtomic.
+template <class W = int, class F>
+void edgeMapReduce(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_t threshold,
+                   const W *w_out = nullptr, const W *w_in = nullptr, bool *took_dense = nullptr) {
+  E.reset_counters();
+  const bool dense = go_dense(cur, threshold);
+  if (took_dense) *took_dense = dense;
+  E.prof.begin(E.tag, E.stream);
+  if (dense) {
+    launch_pull_reduce<W>(E, f, w_in, next.bits, E.d_cnt);
+    next.has_queue = false;
+  } else {
+    launch_sparse_push<W>(E, cur, f, w_out, next);
+  }
+  E.prof.end(E.stream);
+  const Counters *h = E.read_counters();
+  next.size = (int64_t)h[0].size;
+  next.edges = (int64_t)h[0].edges;
+}
+
+template <class F>
+void vertexMap(Engine &E, VertexSubset &s, F f) {
+  PM_LAUNCH((k_vertex_map_bits<F>), E.grid_for(s.n, 256, 16), 256, 0, E.stream, s.n, s.bits, f);
+}
+
+template <class F>
+void vertexMapAll(Engine &E, int32_t n, F f) {
+  PM_LAUNCH((k_vertex_map_all<F>), E.grid_for(n, 256, 16), 256, 0, E.stream, n, f);
+}
+
+template <class F>
+void vertexFilter(Engine &E, VertexSubset &s, F f, VertexSubset &out) {
+  E.reset_counters();
+  int64_t nthreads = ((int64_t)s.n + 31) & ~31ll;
+  PM_LAUNCH((k_vertex_filter<F>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, s.n,
+            E.g.out.off, s.bits, f, out.bits, E.d_cnt);
+  const Counters *h = E.read_counters();
+  out.size = (int64_t)h[0].size;
+  out.edges = (int64_t)h[0].edges;
+  out.has_queue = false;
+}
+
+}  // namespace pm

@@ -1,0 +1,56 @@
+"""CPU tests of the C ABI library: it loads, exports every symbol declared in
+include/polymer_b200.h, and fails loudly (a status, not a crash or a CPU
+fallback) when no GPU is visible.  No compute call runs here."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, have_gpu
+
+HEADER = os.path.join(ROOT, "include", "polymer_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^PM_API\s+[\w\s\*]+?\b(pm_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("pm_graph_create", "pm_bfs", "pm_components", "pm_bellman_ford", "pm_pagerank",
+              "pm_spmv", "pm_bp", "pm_last_error"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    import polymer_b200
+    if not os.path.exists(polymer_b200.LIB_PATH):
+        from polymer_b200 import _build
+        _build.build()
+    L = C.CDLL(polymer_b200.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_version_string():
+    import polymer_b200
+    assert b"sm_100a" in polymer_b200.lib().pm_version()
+
+
+@pytest.mark.skipif(have_gpu(), reason="checks the no-GPU error path")
+def test_no_device_is_an_error_not_a_fallback():
+    import numpy as np
+    import polymer_b200 as pm
+    with pytest.raises(pm.PolymerError) as ei:
+        pm.Graph.from_csr(np.array([0, 1, 1], np.int32), np.array([1], np.int32))
+    assert ei.value.status in (3, 7)  # CUDA error or no device
+    assert pm.lib().pm_last_error()
+
+
+def test_null_handle_is_invalid_arg():
+    import polymer_b200 as pm
+    st = pm.lib().pm_bfs(None, 0, None, None, 0, -1, None)
+    assert st == 1
+    assert b"null graph" in pm.lib().pm_last_error()

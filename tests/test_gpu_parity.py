@@ -1,0 +1,260 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle on
+the same seeded inputs.  Integer results are compared bit-exactly; floating
+point within the tolerances stated per test."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+RTOL_F64 = 1e-10     # PageRank FP64 (reference prints %.9e)
+RL1_F32 = 1e-5       # relative L1 vs the FP64 oracle for FP32 storage/sums
+
+
+def rel_l1(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def dev_graph(pm, og, symmetric=False, skip=False):
+    return pm.Graph.from_csr(og.off, og.idx, symmetric=symmetric, skip_self_loops=skip)
+
+
+def check_parents(og, src, parents, depth):
+    n = og.n
+    assert parents[src] == src and depth[src] == 0
+    reached = depth >= 0
+    assert np.array_equal(reached, parents >= 0)
+    v = np.nonzero(reached & (np.arange(n) != src))[0]
+    p = parents[v]
+    assert np.all(depth[p] == depth[v] - 1), "parent one level up"
+    # the edge p -> v exists in the CSR
+    for a, b in zip(p[:20000], v[:20000]):
+        row = og.idx[og.off[a]:og.off[a + 1]]
+        k = np.searchsorted(row, b)
+        assert k < len(row) and row[k] == b
+
+
+# --------------------------------------------------------------------------
+def test_rmat_generator_matches_oracle(pm, oracle):
+    for scale, ef, sym in ((8, 4, False), (10, 16, True), (14, 16, False), (13, 16, True)):
+        og = oracle.rmat_graph(scale, ef, symmetric=sym)
+        with pm.Graph.rmat(scale, ef, symmetric=sym) as g:
+            off, idx = g.csr()
+            assert g.n == og.n and g.m == og.m
+            assert np.array_equal(off, og.off) and np.array_equal(idx, og.idx)
+
+
+def test_graph_create_skip_self_loops(pm, oracle):
+    z = load("tiny.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"], skip_self_loops=True) as g:
+        off, idx = g.csr()
+    n = len(z["off"]) - 1
+    src = np.repeat(np.arange(n), np.diff(z["off"]))
+    keep = src != z["idx"]
+    og = oracle.graph_from_edges(n, src[keep], z["idx"][keep])
+    assert np.array_equal(off, og.off) and np.array_equal(idx, og.idx)
+
+
+def test_bad_graph_rejected(pm):
+    with pytest.raises(pm.PolymerError) as ei:
+        pm.Graph.from_csr(np.array([0, 2, 1], np.int32), np.array([1, 0], np.int32))
+    assert ei.value.status == 5
+    with pytest.raises(pm.PolymerError):
+        pm.Graph.from_csr(np.array([0, 1, 2], np.int32), np.array([1, 7], np.int32))
+
+
+# --------------------------------------------------------------------------
+def test_pagerank_f64_matches_reference_fixture(pm, oracle):
+    z = load("rmat10_directed.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"]) as g:
+        r = pm.PageRank(g, 10, dtype=np.float64)
+    assert np.allclose(r, z["pagerank10"], rtol=2e-9, atol=0)
+
+
+def test_pagerank_tiny_skip_ring_fixture(pm):
+    z = load("tiny.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"], skip_self_loops=True) as g:
+        r = pm.PageRank(g, 6, dtype=np.float64)
+    assert np.allclose(r, z["pagerank6"], rtol=2e-9, atol=1e-300)
+
+
+def test_pagerank_rejects_self_loops(pm):
+    z = load("tiny.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"]) as g:
+        with pytest.raises(pm.PolymerError):
+            pm.PageRank(g, 3)
+
+
+def test_pagerank_config1_f64(pm, oracle):
+    """2^16 vertices, edge factor 16, 10 iterations, FP64."""
+    og = oracle.rmat_graph(16, 16)
+    ref, res_ref = oracle.pagerank(og, 10, with_resid=True)
+    with pm.Graph.rmat(16, 16) as g:
+        r, res = pm.PageRank(g, 10, dtype=np.float64, resid=True)
+    assert np.allclose(r, ref, rtol=RTOL_F64, atol=0)
+    assert np.allclose(res, res_ref, rtol=1e-9)
+
+
+def test_pagerank_f32_rel_l1(pm, oracle):
+    og = oracle.rmat_graph(18, 16)
+    ref = oracle.pagerank(og, 20)
+    with pm.Graph.rmat(18, 16) as g:
+        r = pm.PageRank(g, 20, dtype=np.float32)
+    assert rel_l1(r, ref) < RL1_F32
+    assert np.max(np.abs(r - ref) / np.maximum(ref, 1e-30)) < 1e-3
+
+
+def test_pagerank_deterministic(pm):
+    with pm.Graph.rmat(14, 16) as g:
+        a = pm.PageRank(g, 7, dtype=np.float32)
+        b = pm.PageRank(g, 7, dtype=np.float32)
+    assert np.array_equal(a, b)
+
+
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+@pytest.mark.parametrize("sym", [True, False])
+def test_bfs_depths_exact(pm, oracle, threshold, sym):
+    og = oracle.rmat_graph(13, 16, symmetric=sym)
+    with dev_graph(pm, og, symmetric=sym) as g:
+        for s in oracle.pick_sources(og, 4, seed=0x5EED0005 + sym):
+            parents, depth = pm.BFS(int(s), g, threshold=threshold)
+            ref, _ = oracle.bfs(og, int(s))
+            assert np.array_equal(depth, ref)
+            check_parents(og, int(s), parents, depth)
+
+
+def test_bfs_reference_fixture(pm, oracle):
+    z = load("rmat10_symmetric.npz")
+    og = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    with dev_graph(pm, og, symmetric=True) as g:
+        for s, par, cnt in zip(z["bfs_sources"], z["bfs_parents"], z["bfs_counts"]):
+            _, depth = pm.BFS(int(s), g, threshold=0)   # the reference's always-dense rule
+            assert np.array_equal(depth, oracle.bfs_depths_from_parents(par, int(s)))
+            assert (depth >= 0).sum() == cnt
+
+
+def test_bfs_isolated_source_and_heavy_rows(pm, oracle):
+    # star: vertex 0 -> 1..5000 (heavy row), 5001 isolated
+    n = 5002
+    og = oracle.graph_from_edges(n, np.zeros(5000, np.int64), np.arange(1, 5001))
+    with dev_graph(pm, og) as g:
+        parents, depth, st = pm.BFS(5001, g, stats=True)
+        assert depth[5001] == 0 and (depth >= 0).sum() == 1 and st["reached"] == 1
+        for thr in (-1, 0):
+            parents, depth = pm.BFS(0, g, threshold=thr)
+            assert np.all(depth[1:5001] == 1) and depth[5001] == -1 and np.all(parents[1:5001] == 0)
+
+
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+def test_components_exact(pm, oracle, threshold):
+    for sym, scale in ((True, 13), (False, 12)):
+        og = oracle.rmat_graph(scale, 8, symmetric=sym)
+        with dev_graph(pm, og, symmetric=sym) as g:
+            lab = pm.Components(g, threshold=threshold)
+        assert np.array_equal(lab, oracle.cc(og))
+
+
+def test_components_reference_fixture(pm, oracle):
+    z = load("rmat10_symmetric.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"], symmetric=True) as g:
+        assert np.array_equal(pm.Components(g), z["cc"])
+
+
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+def test_bellman_ford_exact(pm, oracle, threshold):
+    for sym, scale in ((True, 12), (False, 12)):
+        og = oracle.rmat_graph(scale, 16, symmetric=sym)
+        w = oracle.weights_int(og)
+        with dev_graph(pm, og, symmetric=sym) as g:
+            g.set_weights(w)
+            for s in oracle.pick_sources(og, 3):
+                d = pm.BellmanFord(g, int(s), threshold=threshold)
+                assert np.array_equal(d, oracle.dijkstra(og, w, int(s)))
+
+
+def test_device_weights_match_oracle(pm, oracle):
+    og = oracle.rmat_graph(12, 16, symmetric=True)
+    with pm.Graph.rmat(12, 16, symmetric=True) as g:
+        g.gen_weights_int()
+        assert np.array_equal(g.weights_i32(), oracle.weights_int(og))
+        g.gen_weights_unit()
+        assert np.array_equal(g.weights_f32(), oracle.weights_unit(og))
+
+
+# --------------------------------------------------------------------------
+def test_spmv_integer_weights_reference_fixture(pm):
+    z = load("rmat10_directed.npz")
+    n = len(z["off"]) - 1
+    with pm.Graph.from_csr(z["off"], z["idx"]) as g:
+        g.set_weights(z["spmv_w"].astype(np.float32))
+        y = pm.SPMV(g, np.full(n, 1.0 / n, np.float32), 5)
+    assert rel_l1(y, z["spmv5"]) < RL1_F32
+
+
+def test_spmv_f32_rel_l1(pm, oracle):
+    og = oracle.rmat_graph(16, 16)
+    w = oracle.weights_unit(og)
+    x0 = oracle.uniform01(og.n)
+    ref = oracle.spmv(og, w.astype(np.float64), x0.astype(np.float64), 10)
+    with dev_graph(pm, og) as g:
+        g.set_weights(w)
+        y, norms = pm.SPMV(g, x0, 10, norms=True)
+    assert rel_l1(y, ref) < RL1_F32
+    assert abs(norms[-1] / np.abs(ref).sum() - 1) < RL1_F32
+
+
+# --------------------------------------------------------------------------
+def test_bp_matches_oracle(pm, oracle):
+    og = oracle.rmat_graph(14, 16)
+    prior = oracle.uniform_open(2 * og.n).reshape(og.n, 2)
+    ref = oracle.bp(og, prior.astype(np.float64), 10)
+    with dev_graph(pm, og) as g:
+        out = pm.BeliefPropagation(g, prior, 10)
+    err = np.abs(out - ref).sum() / max(np.abs(ref).sum(), 1e-30)
+    assert err < RL1_F32, err
+
+
+# --------------------------------------------------------------------------
+def test_empty_and_single_vertex_graphs(pm, oracle):
+    with pm.Graph.from_csr(np.array([0, 0], np.int32), np.zeros(0, np.int32)) as g:
+        p, d = pm.BFS(0, g)
+        assert d.tolist() == [0] and p.tolist() == [0]
+        assert pm.Components(g).tolist() == [0]
+        assert np.allclose(pm.PageRank(g, 3), [0.15])
+    off = np.zeros(101, np.int32)
+    with pm.Graph.from_csr(off, np.zeros(0, np.int32)) as g:
+        assert np.array_equal(pm.Components(g), np.arange(100))
+        _, d = pm.BFS(7, g)
+        assert (d >= 0).sum() == 1
+
+
+def test_device_pointers_roundtrip(pm, oracle):
+    import torch
+    og = oracle.rmat_graph(12, 16, symmetric=True)
+    off = torch.from_numpy(og.off).cuda()
+    idx = torch.from_numpy(og.idx).cuda()
+    torch.cuda.synchronize()
+    with pm.Graph.from_csr(off, idx, symmetric=True) as g:
+        lab = pm.Components(g, device_out=off)
+        assert lab.is_cuda and np.array_equal(lab.cpu().numpy(), oracle.cc(og))
+        par, dep = pm.BFS(int(oracle.pick_sources(og, 1)[0]), g, device_out=off)
+        assert dep.is_cuda
+
+
+def test_kernel_launch_counter(pm):
+    with pm.Graph.rmat(10, 8) as g:
+        pm.kernel_launches(reset=True)
+        pm.PageRank(g, 5, dtype=np.float32)
+        assert pm.kernel_launches() >= 5

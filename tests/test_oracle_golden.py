@@ -1,0 +1,133 @@
+"""CPU tests: the oracle restatement against the reference's own outputs.
+
+The fixtures in tests/golden/ were produced by the reference binaries
+(oracle/_ref, built from the original Polymer sources) via
+tests/golden/make_golden.py.  When oracle/_ref is present the reference is
+also run live on fresh graphs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def test_generator_reproduces_fixture_graphs(oracle):
+    z = load("rmat10_directed.npz")
+    g = oracle.rmat_graph(10, 16)
+    assert np.array_equal(g.off, z["off"]) and np.array_equal(g.idx, z["idx"])
+    z = load("rmat10_symmetric.npz")
+    gs = oracle.rmat_graph(10, 16, symmetric=True)
+    assert np.array_equal(gs.off, z["off"]) and np.array_equal(gs.idx, z["idx"])
+
+
+def test_generator_properties(oracle):
+    g = oracle.rmat_graph(12, 16)
+    src = np.repeat(np.arange(g.n), np.diff(g.off))
+    assert np.all(src != g.idx), "self loops must be removed"
+    key = src.astype(np.int64) * g.n + g.idx
+    assert np.all(np.diff(key) > 0), "edges sorted by (src, dst), no duplicates"
+    gs = oracle.rmat_graph(12, 16, symmetric=True)
+    s2 = np.repeat(np.arange(gs.n), np.diff(gs.off))
+    fwd = set(zip(s2.tolist(), gs.idx.tolist()))
+    assert all((b, a) in fwd for a, b in list(fwd)[:5000])
+
+
+def test_pagerank_matches_reference_fixture(oracle):
+    z = load("rmat10_directed.npz")
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    ours = oracle.pagerank(g, 10)
+    ref = z["pagerank10"]
+    # the reference prints %.9e
+    assert np.allclose(ours, ref, rtol=2e-9, atol=0)
+
+
+def test_pagerank_skip_ring_fixture(oracle):
+    z = load("tiny.npz")
+    n = len(z["off"]) - 1
+    src = np.repeat(np.arange(n), np.diff(z["off"]))
+    keep = src != z["idx"]
+    g = oracle.graph_from_edges(n, src[keep], z["idx"][keep])
+    ours = oracle.pagerank(g, 6)
+    assert np.allclose(ours, z["pagerank6"], rtol=2e-9, atol=1e-300)
+
+
+def test_spmv_matches_reference_fixture(oracle):
+    z = load("rmat10_directed.npz")
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    x0 = np.full(g.n, 1.0 / g.n)
+    ours = oracle.spmv(g, z["spmv_w"].astype(np.float64), x0, 5)
+    assert np.allclose(ours, z["spmv5"], rtol=2e-9, atol=0)
+
+
+def test_components_match_reference_fixture(oracle):
+    z = load("rmat10_symmetric.npz")
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    assert np.array_equal(oracle.cc(g), z["cc"])
+
+
+def test_bfs_depths_match_reference_parents(oracle):
+    z = load("rmat10_symmetric.npz")
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    for s, par, cnt in zip(z["bfs_sources"], z["bfs_parents"], z["bfs_counts"]):
+        depth, _ = oracle.bfs(g, int(s))
+        assert np.array_equal(oracle.bfs_depths_from_parents(par, int(s)), depth)
+        assert (depth >= 0).sum() == cnt
+
+
+def test_bellman_ford_is_exact(oracle):
+    for scale, sym in ((10, True), (11, False)):
+        g = oracle.rmat_graph(scale, 8, symmetric=sym)
+        w = oracle.weights_int(g)
+        for s in oracle.pick_sources(g, 3):
+            assert np.array_equal(oracle.bellman_ford(g, w, int(s)), oracle.dijkstra(g, w, int(s)))
+
+
+def test_weights_rules(oracle):
+    g = oracle.rmat_graph(9, 8, symmetric=True)
+    w = oracle.weights_int(g)
+    assert w.min() >= 1 and w.max() <= 22
+    src = np.repeat(np.arange(g.n), np.diff(g.off))
+    lookup = dict(zip(zip(src.tolist(), g.idx.tolist()), w.tolist()))
+    assert all(lookup[(b, a)] == c for (a, b), c in list(lookup.items())[:3000])
+    wu = oracle.weights_unit(g)
+    assert wu.min() > 0 and wu.max() <= 1
+
+
+def test_bp_restatement_small(oracle):
+    # two vertices, one edge 0->1: vertex 1 receives one normalised message
+    g = oracle.graph_from_edges(2, [0], [1])
+    prior = np.array([[0.3, 0.7], [0.6, 0.4]])
+    out = oracle.bp(g, prior, 1)
+    a0, a1 = 0.6, 0.4
+    b0, b1 = 0.9 * a0 + 0.1 * a1, 0.1 * a0 + 0.9 * a1
+    assert np.allclose(out[1], [np.log(b0 / (b0 + b1)), np.log(b1 / (b0 + b1))])
+    assert np.allclose(out[0], [0, 0])
+
+
+def test_depths_from_parents_rejects_cycles(oracle):
+    with pytest.raises(ValueError):
+        oracle.bfs_depths_from_parents(np.array([0, 2, 1], np.int32), 0)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
+                                                    "numa-PageRank")),
+                    reason="reference binaries not built here")
+def test_live_reference_scale12(oracle, tmp_path):
+    g = oracle.rmat_graph(12, 16)
+    base = oracle.write_binary(g, str(tmp_path / "g"))
+    ref, _ = oracle.ref_pagerank(base, 10, threads=4)
+    assert np.allclose(oracle.pagerank(g, 10), ref, rtol=2e-9, atol=0)
+    gs = oracle.rmat_graph(12, 16, symmetric=True)
+    bs = oracle.write_binary(gs, str(tmp_path / "s"))
+    lab, _ = oracle.ref_components(bs, threads=4)
+    assert np.array_equal(lab, oracle.cc(gs))
+    s = int(oracle.pick_sources(gs, 1)[0])
+    par, cnt, _ = oracle.ref_bfs(bs, s, threads=4)
+    depth, _ = oracle.bfs(gs, s)
+    assert np.array_equal(oracle.bfs_depths_from_parents(par, s), depth)
