@@ -74,6 +74,18 @@ __device__ __forceinline__ T shfl_down(T v, int d) {
   }
 }
 
+template <class T>
+__device__ __forceinline__ T shfl_up(T v, int d) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "shuffle of 4/8-byte types only");
+  if constexpr (sizeof(T) == 4) {
+    int x = __shfl_up_sync(0xffffffffu, *reinterpret_cast<int *>(&v), d);
+    return *reinterpret_cast<T *>(&x);
+  } else {
+    long long x = __shfl_up_sync(0xffffffffu, *reinterpret_cast<long long *>(&v), d);
+    return *reinterpret_cast<T *>(&x);
+  }
+}
+
 // Exclusive warp prefix sum of an int; total returned in *total.
 __device__ __forceinline__ int warp_excl_scan(int v, int *total) {
   int lane = lane_id();

@@ -101,16 +101,19 @@ __global__ void k_reverse_eid(const int32_t *off, const int32_t *idx, const int3
 }
 
 // ---- load-balance tables ---------------------------------------------------
-// gstart[g] = first row whose first edge is >= g*kGroupEdges, rounded down
-// to a multiple of 32; gstart[G] = n.
+// Warp groups split the merge path of rows and edges: with the work key
+// key(r) = off[r] + kRowWork * r (strictly increasing), gstart[g] is the
+// first row whose key is >= g * kGroupWork, rounded down to a multiple of 32;
+// gstart[G] = n.  A group therefore holds about kGroupWork units of edges
+// plus rows, however the degrees are distributed.
 __global__ void k_group_starts(const int32_t *off, int64_t n, int32_t G, int32_t *gstart) {
   GRID_STRIDE(g, (int64_t)G + 1) {
     if (g == G) { gstart[g] = (int32_t)n; continue; }
-    int64_t target = g * (int64_t)kGroupEdges;
+    int64_t target = g * (int64_t)kGroupWork;
     int64_t lo = 0, hi = n;
     while (lo < hi) {
       int64_t mid = (lo + hi) >> 1;
-      if (off[mid] < target) lo = mid + 1; else hi = mid;
+      if ((int64_t)off[mid] + (int64_t)kRowWork * mid < target) lo = mid + 1; else hi = mid;
     }
     gstart[g] = (int32_t)(std::min<int64_t>(lo, n) & ~31ll);
   }
@@ -203,7 +206,7 @@ __global__ void k_uniform_f32(uint64_t seed, int open, int64_t count, float *x) 
 // ---------------------------------------------------------------------------
 static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
   const int64_t n = g->n, m = g->m;
-  a.ngroups = (int32_t)((m + kGroupEdges - 1) / kGroupEdges);
+  a.ngroups = (int32_t)((m + kRowWork * n + kGroupWork - 1) / kGroupWork);
   if (a.ngroups < 1) a.ngroups = 1;
   a.gstart.alloc((size_t)(a.ngroups + 1) * 4);
   PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), n, a.ngroups,
@@ -284,10 +287,12 @@ void finish_graph(pm_graph *g) {
   g->queue0.alloc((size_t)(n + 1) * 4);
   g->queue1.alloc((size_t)(n + 1) * 4);
   g->defer.alloc((size_t)(n + 1) * 4);
+  g->hubs.alloc((size_t)kMaxHubs * 4);
   g->partials.alloc((size_t)std::max(v.in.nchunks, 1) * 16);
   g->cnt.alloc(3 * sizeof(Counters));
   g->E.d_cnt = g->cnt.as<Counters>();
   g->E.defer = g->defer.as<int32_t>();
+  g->E.hubs = g->hubs.as<int32_t>();
   g->E.partials = g->partials.p;
   PM_CUDA(cudaStreamSynchronize(st));
 }

@@ -72,7 +72,7 @@ struct pm_graph {
   pm::DevBuf in_eid;      // CSC slot -> CSR edge id (directed graphs)
   pm::DevBuf w_i32_out, w_i32_in, w_f32_out, w_f32_in;
   pm::Engine E;
-  pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, partials;
+  pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials;
   pm::Counters *h_cnt = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<pm::DevBuf> scratch;  // per-call workspaces kept across calls

@@ -36,12 +36,15 @@
 
 namespace pm {
 
-constexpr int kGroupEdges = 1024;  // edge window that defines one warp group
+constexpr int kGroupWork = 1024;   // work units (edges + kRowWork per row) of one warp group
+constexpr int kRowWork = 4;       // a row costs about as much as this many edges
 constexpr int kHeavyDeg = 1024;    // rows above this degree are split in chunks
 constexpr int kChunkEdges = 2048;  // edges of one heavy chunk (one CTA)
 constexpr int kChunkThreads = 256;
 constexpr int kPullScan = 32;      // edges a thread scans before deferring a row
 constexpr int kCtaExpand = 512;    // sparse push: CTA-wide expansion above this degree
+constexpr int kGridExpand = 4096;  // sparse push: rows above this degree use the whole grid
+constexpr int kMaxHubs = 4096;     // hub rows one sparse round can hand to the grid kernel
 
 // One adjacency direction.
 struct Adj {
@@ -117,7 +120,8 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
                                                      int32_t qsize, F f, const W *__restrict__ w,
                                                      int32_t *__restrict__ next_queue,
                                                      uint32_t *__restrict__ next_bits, int32_t qcap,
-                                                     Counters *cnt) {
+                                                     Counters *cnt, int32_t *__restrict__ hubs,
+                                                     Counters *hub_cnt) {
   __shared__ int s_pos[256];
   __shared__ int s_v[256];
   __shared__ int s_o[256];
@@ -130,8 +134,20 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
     int v = -1, o = 0, deg = 0;
     if (i < qsize) {
       v = queue[i];
-      o = __ldg(g.out.off + v);
-      deg = __ldg(g.out.off + v + 1) - o;
+      if (v >= 0 && v < g.n) {
+        o = __ldg(g.out.off + v);
+        deg = __ldg(g.out.off + v + 1) - o;
+      } else {
+        atomicOr(&cnt->err, (unsigned)kErrRange);
+      }
+      // hub rows go to k_sparse_push_hubs, which spreads them over the grid
+      if (deg >= kGridExpand) {
+        unsigned long long slot = atomicAdd(&hub_cnt->size, 1ull);
+        if (slot < (unsigned long long)kMaxHubs) {
+          hubs[slot] = v;
+          deg = 0;
+        }
+      }
     }
     // CTA-wide expansion of long rows.
     for (;;) {
@@ -197,6 +213,82 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
       emit_queue(act, d, next_queue, qcap, cnt);
     }
     __syncthreads();
+  }
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_edges) atomicAdd(&cnt->edges, my_edges);
+}
+
+// Hub rows of a sparse round: every CTA builds the prefix sum of the hubs'
+// degrees in shared memory, then the grid shares their flattened edges, each
+// thread kLaneEdges consecutive ones at a time.
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_sparse_push_hubs(GraphView g, F f, const W *__restrict__ w,
+                                                          const int32_t *__restrict__ hubs,
+                                                          const Counters *hub_cnt,
+                                                          int32_t *__restrict__ next_queue,
+                                                          uint32_t *__restrict__ next_bits,
+                                                          int32_t qcap, Counters *cnt) {
+  constexpr int K = 8;
+  __shared__ int s_pos[kMaxHubs + 1];
+  __shared__ int s_warp[8];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nh = (int)min(hub_cnt->size, (unsigned long long)kMaxHubs);
+  if (nh == 0) return;
+  // exclusive scan of the hub degrees: thread t owns a contiguous slice
+  const int per = (nh + 255) / 256;
+  const int h0 = min(tid * per, nh), h1 = min(h0 + per, nh);
+  int local = 0;
+  for (int h = h0; h < h1; ++h) {
+    const int v = hubs[h];
+    local += __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+  }
+  int wtot;
+  int pre = warp_excl_scan(local, &wtot);
+  if (lane == 0) s_warp[wid] = wtot;
+  __syncthreads();
+  int base = 0, total = 0;
+  for (int k = 0; k < 8; ++k) {
+    if (k < wid) base += s_warp[k];
+    total += s_warp[k];
+  }
+  int run = base + pre;
+  for (int h = h0; h < h1; ++h) {
+    s_pos[h] = run;
+    const int v = hubs[h];
+    run += __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+  }
+  if (tid == 0) s_pos[nh] = total;
+  __syncthreads();
+  unsigned long long my_edges = 0;
+  const int64_t stride = (int64_t)gridDim.x * 256 * K;
+  for (int64_t q0 = ((int64_t)blockIdx.x * 256 + tid) * K; q0 - tid * K < total; q0 += stride) {
+    int h = 0;
+    if (q0 < total) {  // last hub whose flat start is <= q0
+      int lo = 0, hi = nh - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pos[mid] <= q0) lo = mid; else hi = mid - 1;
+      }
+      h = lo;
+    }
+    int v = q0 < total ? hubs[h] : 0;
+    int64_t o = q0 < total ? (int64_t)__ldg(g.out.off + v) : 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t q = q0 + k;
+      int d = -1;
+      bool act = false;
+      if (q < total) {
+        while (q >= s_pos[h + 1]) {
+          ++h;
+          v = hubs[h];
+          o = __ldg(g.out.off + v);
+        }
+        act = push_edge(g, f, w, v, o + (q - s_pos[h]), next_bits, d);
+      }
+      if (act) my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
+      emit_queue(act, d, next_queue, qcap, cnt);
+    }
   }
   my_edges = warp_sum(my_edges);
   if (lane == 0 && my_edges) atomicAdd(&cnt->edges, my_edges);
@@ -300,15 +392,20 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
 
 // ---------------------------------------------------------------------------
 // Dense pull-reduce (edgeMapDenseReduce, polymer.h:1097-1168).  A warp takes
-// one group: the 32-aligned rows whose first in-edge falls in a window of
-// kGroupEdges edges.  It walks them 32 rows at a time, lays their edges out
-// flat (consecutive rows are consecutive in the CSC, so loads coalesce),
-// evaluates f.edge() per edge, folds each row with a segmented warp
-// reduction into shared memory and lets the row's lane run f.commit() (the
-// fused vertexMap).  Rows with more than kHeavyDeg edges are reduced first
-// by k_heavy_reduce (one CTA per kChunkEdges chunk) into partials[], which
-// the owning lane folds in chunk order -- every result is deterministic.
+// one group: about kGroupWork units of rows and edges on the merge path
+// (32-aligned row ranges).  It walks them 32 rows at a time and lays their edges
+// out flat (consecutive rows are consecutive in the CSC).  Each lane takes
+// kLaneEdges consecutive flat edges per window: it issues all their id loads
+// and f.edge() gathers before folding any, which keeps kLaneEdges loads in
+// flight per lane, folds them locally per row, stores rows that start and
+// end inside it, and hands its first / last partial row to a segmented warp
+// reduction keyed by row.  Row sums collect in shared memory; the row's lane
+// then runs f.commit() (the fused vertexMap).  Rows with more than kHeavyDeg
+// edges are reduced first by k_heavy_reduce (one CTA per kChunkEdges chunk)
+// into partials[], which the owning lane folds in chunk order.  The order of
+// every reduction is fixed, so results are deterministic.
 // ---------------------------------------------------------------------------
+constexpr int kLaneEdges = 8;
 template <class F, class W>
 __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f,
                                                                 const W *__restrict__ w,
@@ -323,8 +420,19 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f
   const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.in.off + r + 1));
   Acc acc = f.identity();
   if (f.cond(r)) {
-    for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads)
-      acc = f.combine(acc, f.edge(__ldg(g.in.idx + e), r, load_w(w, e)));
+    static_assert(kChunkEdges % kChunkThreads == 0, "chunk must be a multiple of the CTA");
+    constexpr int U = kChunkEdges / kChunkThreads;
+    int src[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t e = e0 + threadIdx.x + (int64_t)u * kChunkThreads;
+      src[u] = e < e1 ? __ldg(g.in.idx + e) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t e = e0 + threadIdx.x + (int64_t)u * kChunkThreads;
+      if (e < e1) acc = f.combine(acc, f.edge(src[u], r, load_w(w, e)));
+    }
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) acc = f.combine(acc, shfl_down(acc, d));
@@ -342,10 +450,16 @@ __global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *
                                                      const typename F::Acc *__restrict__ partials,
                                                      uint32_t *__restrict__ next, Counters *cnt) {
   using Acc = typename F::Acc;
+  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges;
   __shared__ Acc s_acc[8][32];
+  __shared__ int s_pos[8][33];
+  __shared__ int s_off[8][32];
   const int lane = lane_id(), wid = threadIdx.x >> 5;
   const int grp = blockIdx.x * 8 + wid;
   if (grp >= g.in.ngroups) return;
+  Acc *acc_s = s_acc[wid];
+  int *pos_s = s_pos[wid];
+  int *off_s = s_off[wid];
   const int r_begin = __ldg(g.in.gstart + grp), r_end = __ldg(g.in.gstart + grp + 1);
   unsigned long long my_size = 0, my_edges = 0;
   double my_aux = 0.0;
@@ -363,27 +477,69 @@ __global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *
     const int ldeg = (live && !heavy) ? deg : 0;
     int total;
     const int pos = warp_excl_scan(ldeg, &total);
-    s_acc[wid][lane] = f.identity();
+    pos_s[lane] = pos;
+    if (lane == 31) pos_s[32] = total;
+    off_s[lane] = o0;
+    acc_s[lane] = f.identity();
     __syncwarp();
-    for (int c = 0; c < total; c += 32) {
-      const int q = c + lane;
-      const bool active = q < total;
-      // owner lane j: the last lane whose flat start is <= q
+    for (int c = 0; c < total; c += WIN) {
+      const int q0 = c + lane * K;
+      const bool active = q0 < total;
+      // row (lane index j) and CSC slot of each of this lane's K flat edges
       int j = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        int cand = j + step;
-        int pc = __shfl_sync(0xffffffffu, pos, cand);
-        if (pc <= q) j = cand;
-      }
-      const int oj = __shfl_sync(0xffffffffu, o0, j);
-      const int pj = __shfl_sync(0xffffffffu, pos, j);
-      Acc v = f.identity();
       if (active) {
-        const int64_t e = (int64_t)oj + (q - pj);
-        v = f.edge(__ldg(g.in.idx + e), rb + j, load_w(w, e));
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (pos_s[j + step] <= q0) j += step;
       }
-      const int key = active ? j : 32 + lane;
+      int rows[K], es[K], src[K];
+      int nxt = pos_s[j + 1];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int q = q0 + k;
+        if (q < total)
+          while (q >= nxt) nxt = pos_s[++j + 1];
+        rows[k] = j;
+        es[k] = off_s[j] + (q - pos_s[j]);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? __ldg(g.in.idx + es[k]) : 0;
+      Acc vals[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        vals[k] = (q0 + k < total) ? f.edge(src[k], rb + rows[k], load_w(w, es[k])) : f.identity();
+      // Local fold: the first segment is the head, rows that start and end
+      // inside the lane are stored directly, the last segment is the tail.
+      Acc head = f.identity(), run = f.identity();
+      int jr = rows[0];
+      bool split = false;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (q0 + k < total) {
+          if (rows[k] != jr) {
+            if (!split) {
+              head = run;
+              split = true;
+            } else {
+              acc_s[jr] = f.combine(acc_s[jr], run);
+            }
+            run = f.identity();
+            jr = rows[k];
+          }
+          run = f.combine(run, vals[k]);
+        }
+      }
+      Acc tail = f.identity();
+      if (split) tail = run; else head = run;
+      const int jf = rows[0], jl = jr;
+      // the previous lane's tail continues into this lane's head
+      const int p_jl = __shfl_up_sync(0xffffffffu, jl, 1);
+      const int p_split = __shfl_up_sync(0xffffffffu, (int)(split && active), 1);
+      const Acc p_tail = shfl_up(tail, 1);
+      if (active && lane > 0 && p_split && p_jl == jf) head = f.combine(p_tail, head);
+      // segmented suffix reduction of the heads, keyed by row
+      const int key = active ? jf : 64 + lane;
+      Acc v = head;
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
         Acc t = shfl_down(v, d);
@@ -391,10 +547,13 @@ __global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *
         if (lane + d < 32 && tk == key) v = f.combine(v, t);
       }
       const int prev_key = __shfl_up_sync(0xffffffffu, key, 1);
-      if (active && (lane == 0 || prev_key != key)) s_acc[wid][j] = f.combine(s_acc[wid][j], v);
+      const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
+      if (active && (lane == 0 || prev_key != key)) acc_s[jf] = f.combine(acc_s[jf], v);
+      // a tail that the next lane does not continue is complete here
+      if (active && split && (lane == 31 || next_key != jl)) acc_s[jl] = f.combine(acc_s[jl], tail);
       __syncwarp();
     }
-    Acc acc = s_acc[wid][lane];
+    Acc acc = acc_s[lane];
     if (live && heavy) {
       const int first = __ldg(g.in.hfirst + r);
       const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
@@ -624,6 +783,7 @@ struct Engine {
   Counters *d_cnt = nullptr;   // [0] next frontier, [1] deferred rows, [2] aux
   Counters *h_cnt = nullptr;   // pinned mirror
   int32_t *defer = nullptr;    // n
+  int32_t *hubs = nullptr;     // kMaxHubs
   void *partials = nullptr;    // max(in.nchunks, 1) * 16 bytes
   int num_sms = 148;
   Profiler prof;
@@ -676,7 +836,9 @@ void launch_sparse_push(Engine &E, VertexSubset &cur, F f, const W *w_out, Verte
   if (cur.size > 0) {
     int grid = E.grid_for(cur.size, 256, 8);
     PM_LAUNCH((k_sparse_push<F, W>), grid, 256, 0, E.stream, E.g, cur.queue, (int32_t)cur.size, f,
-              w_out, next.queue, next.bits, next.n, E.d_cnt);
+              w_out, next.queue, next.bits, next.n, E.d_cnt, E.hubs, E.d_cnt + 1);
+    PM_LAUNCH((k_sparse_push_hubs<F, W>), E.num_sms * 4, 256, 0, E.stream, E.g, f, w_out, E.hubs,
+              E.d_cnt + 1, next.queue, next.bits, next.n, E.d_cnt);
   }
   next.has_queue = true;
 }

@@ -150,9 +150,32 @@ def test_bfs_isolated_source_and_heavy_rows(pm, oracle):
     with dev_graph(pm, og) as g:
         parents, depth, st = pm.BFS(5001, g, stats=True)
         assert depth[5001] == 0 and (depth >= 0).sum() == 1 and st["reached"] == 1
-        for thr in (-1, 0):
+        for thr in (-1, 0, 1 << 40):
             parents, depth = pm.BFS(0, g, threshold=thr)
             assert np.all(depth[1:5001] == 1) and depth[5001] == -1 and np.all(parents[1:5001] == 0)
+
+
+def test_bfs_sparse_hubs(pm, oracle):
+    """Forced sparse rounds on a graph whose hubs exceed the grid-expansion
+    degree, and a complete bipartite graph with more hubs than one round can
+    hand to the grid kernel (the rest take the CTA path)."""
+    og = oracle.rmat_graph(16, 16, symmetric=True)
+    assert og.out_degree().max() > 4096
+    with dev_graph(pm, og, symmetric=True) as g:
+        for s in oracle.pick_sources(og, 3, seed=99):
+            parents, depth = pm.BFS(int(s), g, threshold=1 << 40)
+            assert np.array_equal(depth, oracle.bfs(og, int(s))[0])
+            check_parents(og, int(s), parents, depth)
+    a = 4100
+    left = np.repeat(np.arange(a), a)
+    right = np.tile(np.arange(a, 2 * a), a)
+    kb = oracle.graph_from_edges(2 * a, left, right, symmetric=True)
+    with dev_graph(pm, kb, symmetric=True) as g:
+        for thr in (1 << 40, -1):
+            parents, depth, st = pm.BFS(0, g, threshold=thr, stats=True)
+            assert np.all(depth[1:a] == 2) and np.all(depth[a:] == 1) and depth[0] == 0
+            assert st["reached"] == 2 * a
+            assert np.all((parents[1:a] >= a)) and np.all(parents[a:] == 0)
 
 
 # --------------------------------------------------------------------------
