@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--scale-a", type=int, default=22)
     p.add_argument("--scale-b", type=int, default=24)
     p.add_argument("--sources", type=int, default=16)
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
@@ -199,61 +199,73 @@ class Suite:
 
 def e2e_run(pm, suite, steps):
     """Suite through the public API from pinned host CSR arrays, per step:
-    upload + build both graphs, set weights, run, read every result back."""
+    upload + build both graphs, set weights, run, read every result back
+    into preallocated pinned host buffers."""
     A, B = suite.A, suite.B
-    hA = {k: pm.PinnedArray(c, t) for k, (c, t) in
-          {"off": (A.n + 1, np.int32), "idx": (A.m, np.int32), "w": (A.m, np.int32)}.items()}
-    hB = {k: pm.PinnedArray(c, t) for k, (c, t) in
-          {"off": (B.n + 1, np.int32), "idx": (B.m, np.int32), "w": (B.m, np.float32),
-           "x0": (B.n, np.float32), "prior": (2 * B.n, np.float32)}.items()}
-    oA, iA = A.csr()
-    hA["off"].array[:] = oA
-    hA["idx"].array[:] = iA
+    pin = lambda c, t: pm.PinnedArray(c, t)
+    hA = {"off": pin(A.n + 1, np.int32), "idx": pin(A.m, np.int32), "w": pin(A.m, np.int32)}
+    hB = {"off": pin(B.n + 1, np.int32), "idx": pin(B.m, np.int32), "w": pin(B.m, np.float32),
+          "x0": pin(B.n, np.float32), "prior": pin(2 * B.n, np.float32)}
+    ns = len(suite.sources)
+    oA = {"par": [pin(A.n, np.int32) for _ in range(ns)], "dep": [pin(A.n, np.int32) for _ in range(ns)],
+          "lab": pin(A.n, np.int32), "dist": pin(A.n, np.int32)}
+    oB = {"rank": pin(B.n, np.float32), "y": pin(B.n, np.float32), "lp": pin(2 * B.n, np.float32)}
+    offA, idxA = A.csr()
+    hA["off"].array[:] = offA
+    hA["idx"].array[:] = idxA
     hA["w"].array[:] = A.weights_i32()
-    oB, iB = B.csr()
-    hB["off"].array[:] = oB
-    hB["idx"].array[:] = iB
+    offB, idxB = B.csr()
+    hB["off"].array[:] = offB
+    hB["idx"].array[:] = idxB
     hB["w"].array[:] = B.weights_f32()
     hB["x0"].array[:] = suite.x0.cpu().numpy()
     hB["prior"].array[:] = suite.prior.cpu().numpy().reshape(-1)
     h2d = sum(a.array.nbytes for a in hA.values()) + sum(a.array.nbytes for a in hB.values())
-    d2h = 0
-    times, edges = [], 0
+    d2h = sum(a.array.nbytes for a in oA["par"] + oA["dep"]) + oA["lab"].array.nbytes + \
+        oA["dist"].array.nbytes + sum(a.array.nbytes for a in oB.values())
+    times, phases, edges = [], [], 0
     for _ in range(steps):
         suite.torch.cuda.synchronize()
         t0 = time.perf_counter()
         e = 0
-        d2h = 0
         with pm.Graph.from_csr(hA["off"].array, hA["idx"].array, symmetric=True) as gA:
             gA.set_weights(hA["w"].array)
-            for s in suite.sources:
-                p, d, st = pm.BFS(s, gA, stats=True)
+            t1 = time.perf_counter()
+            for k, s in enumerate(suite.sources):
+                _, _, st = pm.BFS(s, gA, stats=True, out=(oA["par"][k].array, oA["dep"][k].array))
                 e += st["edges_visited"]
-                d2h += p.nbytes + d.nbytes
-            lab = pm.Components(gA)
-            dist = pm.BellmanFord(gA, suite.sources[0])
+            pm.Components(gA, out=oA["lab"].array)
+            pm.BellmanFord(gA, suite.sources[0], out=oA["dist"].array)
             e += 2 * gA.m
-            d2h += lab.nbytes + dist.nbytes
+            t2 = time.perf_counter()
+        t3 = time.perf_counter()
         with pm.Graph.from_csr(hB["off"].array, hB["idx"].array) as gB:
             gB.set_weights(hB["w"].array)
-            r = pm.PageRank(gB, 20, dtype=np.float32)
-            y = pm.SPMV(gB, hB["x0"].array, 10)
-            lp = pm.BeliefPropagation(gB, hB["prior"].array.reshape(-1, 2), 10)
+            t4 = time.perf_counter()
+            pm.PageRank(gB, 20, dtype=np.float32, out=oB["rank"].array)
+            pm.SPMV(gB, hB["x0"].array, 10, out=oB["y"].array)
+            pm.BeliefPropagation(gB, hB["prior"].array.reshape(-1, 2), 10, out=oB["lp"].array)
             e += gB.m * 40
-            d2h += r.nbytes + y.nbytes + lp.nbytes
-        times.append(time.perf_counter() - t0)
+            t5 = time.perf_counter()
+        t6 = time.perf_counter()
+        times.append(t6 - t0)
+        phases.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4, t6 - t5])
         edges = e
-    for a in list(hA.values()) + list(hB.values()):
+    for a in list(hA.values()) + list(hB.values()) + oA["par"] + oA["dep"] + [oA["lab"], oA["dist"]] + \
+            list(oB.values()):
         a.free()
-    t = statistics.median(times)
+    i = int(np.argsort(times)[len(times) // 2])
+    t = times[i]
+    names = ["build_A", "run_A", "free_A", "build_B", "run_B", "free_B"]
     return {"value": round(edges / t / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t, 4),
+            "phases_s": {k: round(v, 4) for k, v in zip(names, phases[i])},
             "timing": "host clock around synchronous API calls, median of %d steps" % steps}
 
 
 def ncu_traffic():
     """DRAM bytes per PageRank pass from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "pagerank_pull_scale24.md")
+    path = os.path.join(ROOT, "profiles", "pagerank_pull_rmat24.md")
     try:
         for ln in open(path):
             if ln.strip().startswith("traffic_bytes_per_pass:"):

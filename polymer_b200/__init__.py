@@ -258,8 +258,17 @@ class PinnedArray:
             pass
 
 
-def _out(like, n, dtype):
-    """Output buffer in the memory space of `like` (torch CUDA tensor) or numpy."""
+def _out(like, n, dtype, out=None):
+    """Output buffer: `out` if given (numpy array or CUDA tensor of n items),
+    else a new one in the memory space of `like` (CUDA tensor) or numpy."""
+    if out is not None:
+        if _is_device(out):
+            if out.numel() != n or out.element_size() != np.dtype(dtype).itemsize:
+                raise PolymerError(1, "out must hold %d items of %s" % (n, np.dtype(dtype).name))
+            return out, C.c_void_p(out.data_ptr()), PM_MEM_DEVICE
+        if out.size != n or out.dtype != np.dtype(dtype) or not out.flags.c_contiguous:
+            raise PolymerError(1, "out must be a contiguous %s array of %d items" % (np.dtype(dtype).name, n))
+        return out, out.ctypes.data_as(C.c_void_p), PM_MEM_HOST
     if like is not None and _is_device(like):
         import torch
         t = torch.empty(n, dtype={np.int32: torch.int32, np.float32: torch.float32,
@@ -269,37 +278,41 @@ def _out(like, n, dtype):
     return a, a.ctypes.data_as(C.c_void_p), PM_MEM_HOST
 
 
-def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool = False):
+def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool = False, out=None):
     """Parents and depths from `start` (numa-BFS.C BFS_F).  threshold < 0:
-    direction switch at m/20; 0: dense pull every level as the reference."""
-    par, pp, mem = _out(device_out, g.n, np.int32)
-    dep, pd, _ = _out(device_out, g.n, np.int32)
+    direction switch at m/20; 0: dense pull every level as the reference.
+    out: optional (parents, depth) buffers to write into."""
+    par, pp, mem = _out(device_out, g.n, np.int32, None if out is None else out[0])
+    dep, pd, mem2 = _out(device_out, g.n, np.int32, None if out is None else out[1])
+    if mem != mem2:
+        raise PolymerError(1, "parents and depth must live in the same memory space")
     st = TraversalStats()
     _check(lib().pm_bfs(g.handle, int(start), pp, pd, mem, int(threshold), C.byref(st)))
     return (par, dep, st.as_dict()) if stats else (par, dep)
 
 
-def Components(g: Graph, threshold: int = -1, device_out=None, stats: bool = False):
+def Components(g: Graph, threshold: int = -1, device_out=None, stats: bool = False, out=None):
     """Min-label connected components (numa-Components.C CC_F)."""
-    lab, pl, mem = _out(device_out, g.n, np.int32)
+    lab, pl, mem = _out(device_out, g.n, np.int32, out)
     st = TraversalStats()
     _check(lib().pm_components(g.handle, pl, mem, int(threshold), C.byref(st)))
     return (lab, st.as_dict()) if stats else lab
 
 
-def BellmanFord(g: Graph, start: int, threshold: int = -1, device_out=None, stats: bool = False):
+def BellmanFord(g: Graph, start: int, threshold: int = -1, device_out=None, stats: bool = False,
+                out=None):
     """Shortest-path distances over the int32 weights (numa-BellmanFord.C BF_F)."""
-    dist, pd, mem = _out(device_out, g.n, np.int32)
+    dist, pd, mem = _out(device_out, g.n, np.int32, out)
     st = TraversalStats()
     _check(lib().pm_bellman_ford(g.handle, int(start), pd, mem, int(threshold), C.byref(st)))
     return (dist, st.as_dict()) if stats else dist
 
 
 def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float64,
-             device_out=None, resid: bool = False):
+             device_out=None, resid: bool = False, out=None):
     """Polymer-semantics PageRank (numa-PageRank.C PR_F); dtype float32/float64."""
     dt = np.float64 if np.dtype(dtype) == np.float64 else np.float32
-    ranks, pr, mem = _out(device_out, g.n, dt)
+    ranks, pr, mem = _out(device_out, g.n, dt, out)
     res = np.zeros(max(maxIter, 1), np.float64)
     _check(lib().pm_pagerank(g.handle, int(maxIter), float(damping),
                              PM_F64 if dt == np.float64 else PM_F32, pr, mem,
@@ -307,17 +320,19 @@ def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float6
     return (ranks, res[:maxIter]) if resid else ranks
 
 
-def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False):
+def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False, out=None):
     """x <- A_w^T x, maxIter times, over the float weights (numa-SPMV.C SPMV_F)."""
     px, mem, keep = _arg(x0, np.float32)
-    y, py, _ = _out(x0 if mem == PM_MEM_DEVICE else None, g.n, np.float32)
+    y, py, mem2 = _out(x0 if mem == PM_MEM_DEVICE else None, g.n, np.float32, out)
+    if mem != mem2:
+        raise PolymerError(1, "x0 and out must live in the same memory space")
     nrm = np.zeros(max(maxIter, 1), np.float64)
     _check(lib().pm_spmv(g.handle, px, int(maxIter), py, mem,
                          nrm.ctypes.data_as(C.c_void_p) if norms else None))
     return (y, nrm[:maxIter]) if norms else y
 
 
-def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1, 0.9))):
+def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1, 0.9)), out=None):
     """2-state BP log-products (n x 2) (numa-BP.C BP_F, normalised messages)."""
     pp, mem, keep = _arg(prior, np.float32)
     psi_a = np.ascontiguousarray(psi, np.float32).reshape(4)
@@ -328,9 +343,12 @@ def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1,
     else:
         psi_t = psi_a
         ppsi = psi_a.ctypes.data_as(C.c_void_p)
-    out, po, _ = _out(prior if mem == PM_MEM_DEVICE else None, 2 * g.n, np.float32)
+    flat = None if out is None else out.reshape(-1)
+    res, po, mem2 = _out(prior if mem == PM_MEM_DEVICE else None, 2 * g.n, np.float32, flat)
+    if mem != mem2:
+        raise PolymerError(1, "prior and out must live in the same memory space")
     _check(lib().pm_bp(g.handle, pp, ppsi, int(maxIter), po, mem))
-    return out.reshape(g.n, 2)
+    return res.reshape(g.n, 2)
 
 
 def uniform_f32(g: Graph, count: int, seed: int, open_interval: bool = False):

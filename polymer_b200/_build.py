@@ -62,6 +62,15 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
+def build_gather_probe() -> str:
+    """Standalone gather-rate probe (csrc/gather_probe.cu) -> polymer_b200/gather_probe."""
+    exe = os.path.join(PKG, "gather_probe")
+    src = os.path.join(CSRC, "gather_probe.cu")
+    if _stale(exe, [src]):
+        subprocess.run([_nvcc(), *ARCH, "-O3", "-o", exe, src], check=True)
+    return exe
+
+
 if __name__ == "__main__":
     build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_info="--ptxas" in sys.argv)
     print(LIB)

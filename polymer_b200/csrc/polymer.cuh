@@ -38,8 +38,8 @@ namespace pm {
 
 constexpr int kGroupWork = 1024;   // work units (edges + kRowWork per row) of one warp group
 constexpr int kRowWork = 4;       // a row costs about as much as this many edges
-constexpr int kHeavyDeg = 1024;    // rows above this degree are split in chunks
-constexpr int kChunkEdges = 2048;  // edges of one heavy chunk (one CTA)
+constexpr int kHeavyDeg = 2048;    // rows above this degree are split in chunks
+constexpr int kChunkEdges = 4096;  // edges of one heavy chunk (one CTA)
 constexpr int kChunkThreads = 256;
 constexpr int kPullScan = 32;      // edges a thread scans before deferring a row
 constexpr int kCtaExpand = 512;    // sparse push: CTA-wide expansion above this degree
@@ -405,7 +405,14 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
 // into partials[], which the owning lane folds in chunk order.  The order of
 // every reduction is fixed, so results are deterministic.
 // ---------------------------------------------------------------------------
-constexpr int kLaneEdges = 8;
+#ifndef PM_LANE_EDGES
+#define PM_LANE_EDGES 8
+#endif
+#ifndef PM_PULL_BLOCK
+#define PM_PULL_BLOCK 256
+#endif
+constexpr int kLaneEdges = PM_LANE_EDGES;
+constexpr int kPullBlock = PM_PULL_BLOCK;
 template <class F, class W>
 __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f,
                                                                 const W *__restrict__ w,
@@ -446,23 +453,27 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f
 }
 
 template <class F, class W>
-__global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
+__global__ void __launch_bounds__(kPullBlock) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
                                                      const typename F::Acc *__restrict__ partials,
                                                      uint32_t *__restrict__ next, Counters *cnt) {
   using Acc = typename F::Acc;
-  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges;
-  __shared__ Acc s_acc[8][32];
-  __shared__ int s_pos[8][33];
-  __shared__ int s_off[8][32];
+  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges, NW = kPullBlock / 32;
+  __shared__ Acc s_acc[NW][32];
+  __shared__ int s_pos[NW][33];
+  __shared__ int s_off[NW][32];
   const int lane = lane_id(), wid = threadIdx.x >> 5;
-  const int grp = blockIdx.x * 8 + wid;
-  if (grp >= g.in.ngroups) return;
   Acc *acc_s = s_acc[wid];
   int *pos_s = s_pos[wid];
   int *off_s = s_off[wid];
-  const int r_begin = __ldg(g.in.gstart + grp), r_end = __ldg(g.in.gstart + grp + 1);
   unsigned long long my_size = 0, my_edges = 0;
   double my_aux = 0.0;
+  // persistent warps: each takes the next group from a ticket counter
+  for (;;) {
+  int grp = 0;
+  if (lane == 0) grp = (int)atomicAdd(&cnt->aux, 1ull);
+  grp = __shfl_sync(0xffffffffu, grp, 0);
+  if (grp >= g.in.ngroups) break;
+  const int r_begin = __ldg(g.in.gstart + grp), r_end = __ldg(g.in.gstart + grp + 1);
   for (int rb = r_begin; rb < r_end; rb += 32) {
     const int r = rb + lane;
     const bool valid = r < r_end;
@@ -494,13 +505,45 @@ __global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *
       }
       int rows[K], es[K], src[K];
       int nxt = pos_s[j + 1];
+      // all K edges of this lane lie in row j (nxt <= total)
+      const bool single = active && q0 + K <= nxt;
+      // ... and every active lane lies in lane 0's row: one row spans the window
+      const int j0 = __shfl_sync(0xffffffffu, j, 0);
+      const bool uniform = __all_sync(0xffffffffu, !active || (single && j == j0));
+      if (uniform) {
+        // The window's edges are one contiguous run of row j0: read them
+        // lane-strided (one 128-byte line per load) and reduce the warp.
+        const int e0 = off_s[j0] + (c - pos_s[j0]);
+        const int cnt = min(WIN, total - c);
+        Acc s = f.identity();
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int q = q0 + k;
-        if (q < total)
-          while (q >= nxt) nxt = pos_s[++j + 1];
-        rows[k] = j;
-        es[k] = off_s[j] + (q - pos_s[j]);
+        for (int k = 0; k < K; ++k)
+          src[k] = (32 * k + lane < cnt) ? __ldg(g.in.idx + e0 + 32 * k + lane) : 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (32 * k + lane < cnt) s = f.combine(s, f.edge(src[k], rb + j0, load_w(w, (int64_t)e0 + 32 * k + lane)));
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) s = f.combine(s, shfl_down(s, d));
+        if (lane == 0) acc_s[j0] = f.combine(acc_s[j0], s);
+        __syncwarp();
+        continue;
+      }
+      if (single) {
+        const int e0 = off_s[j] + (q0 - pos_s[j]);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          rows[k] = j;
+          es[k] = e0 + k;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int q = q0 + k;
+          if (q < total)
+            while (q >= nxt) nxt = pos_s[++j + 1];
+          rows[k] = j;
+          es[k] = off_s[j] + (q - pos_s[j]);
+        }
       }
 #pragma unroll
       for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? __ldg(g.in.idx + es[k]) : 0;
@@ -568,6 +611,7 @@ __global__ void __launch_bounds__(256) k_pull_reduce(GraphView g, F f, const W *
     }
     __syncwarp();
   }
+  }  // group loop
   my_size = warp_sum(my_size);
   my_edges = warp_sum(my_edges);
   my_aux = warp_sum(my_aux);
@@ -874,8 +918,16 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
   if (E.g.in.nchunks > 0)
     PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in,
               partials);
-  PM_LAUNCH((k_pull_reduce<F, W>), (E.g.in.ngroups + 7) / 8, 256, 0, E.stream, E.g, f, w_in,
-            (const Acc *)partials, next_bits, cnt);
+  // persistent grid: as many CTAs as fit on the device at once
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull_reduce<F, W>, kPullBlock, 0));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int64_t want = ((int64_t)E.g.in.ngroups + kPullBlock / 32 - 1) / (kPullBlock / 32);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)E.num_sms * per_sm));
+  PM_LAUNCH((k_pull_reduce<F, W>), grid, kPullBlock, 0, E.stream, E.g, f, w_in, (const Acc *)partials,
+            next_bits, cnt);
 }
 
 // edgeMap (polymer.h:2240-2309): sparse push below the threshold, otherwise
