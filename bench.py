@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
     return p.parse_args()
 
 
@@ -261,6 +262,30 @@ def e2e_run(pm, suite, steps):
             "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t, 4),
             "phases_s": {k: round(v, 4) for k, v in zip(names, phases[i])},
             "timing": "host clock around synchronous API calls, median of %d steps" % steps}
+
+
+def batched_block(pm, suite, reps=3):
+    """configs[3] workloads against plain runs on the same GPU: 64-source BFS
+    (uint64 lanes) vs 64 single-source BFS; device time by CUDA events."""
+    A = suite.A
+    offA, _ = A.csr()
+    src64 = suite._pick_sources(offA, 64, SEED_SRC + 100)
+    out = suite.torch.empty((64, A.n), dtype=suite.torch.int32, device=suite.dev)
+    pm.BFSMulti(src64, A, device_out=out, out=out)
+    ms_multi, st = [], None
+    for _ in range(reps):
+        A.timer_begin()
+        _, st = pm.BFSMulti(src64, A, device_out=out, out=out, stats=True)
+        ms_multi.append(A.timer_end())
+    ms_plain = 0.0
+    for s in src64:
+        A.timer_begin()
+        pm.BFS(s, A, device_out=suite.outA)
+        ms_plain += A.timer_end()
+    t = statistics.median(ms_multi)
+    return {"bfs64": {"ms": round(t, 3), "gteps": round(st["edges_visited"] / (t / 1e3) / 1e9, 2),
+                      "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
+                      "graph": "symmetrised R-MAT scale %d" % int(np.log2(A.n))}}
 
 
 def ncu_traffic():
@@ -514,6 +539,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline()
         except Exception as exc:  # keep the GPU line even if the CPU sample fails
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    if not args.no_batched:
+        line["batched"] = batched_block(pm, suite)
     if not args.no_e2e:
         line["e2e"] = e2e_run(pm, suite, args.e2e_steps)
     if dist:

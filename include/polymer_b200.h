@@ -120,6 +120,17 @@ typedef struct pm_traversal_stats {
 PM_API pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
                  int64_t threshold, pm_traversal_stats *stats);
 
+/* Multi-source BFS: k <= 64 sources in one traversal, one bit per source in
+ * a uint64 word per vertex (BFS_F of numa-BFS.C:59-79 with the parent CAS
+ * replaced by per-source visited bits; the reference runs one BFS per
+ * process).  depth: k*n int32, source-major (depth[l*n + v] = level of v from
+ * sources[l], -1 when unreached) -- each row equals pm_bfs's depth for that
+ * source.  sources: k int32 in mem's space.  stats->reached = sum over
+ * sources of reached vertices; stats->edges_visited = sum over sources of the
+ * out-degrees of the reached vertices. */
+PM_API pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *depth,
+                              uint32_t mem, int64_t threshold, pm_traversal_stats *stats);
+
 /* Connected components by min-label propagation.  Replaces Components(GA)
  * (numa-Components.C:402) with CC_F / CC_Vertex_F (55-119): labels start at
  * the vertex id, every round lowers labels along the out-edges of the

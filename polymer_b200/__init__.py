@@ -24,7 +24,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "Graph", "PolymerError", "PageRank", "BFS", "Components", "BellmanFord", "SPMV",
+    "Graph", "PolymerError", "PageRank", "BFS", "BFSMulti", "Components", "BellmanFord", "SPMV",
     "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
 ]
 
@@ -81,6 +81,7 @@ def lib():
         "pm_graph_get_weights_i32": [vp, vp, u32],
         "pm_fill_uniform_f32": [vp, u64, C.c_int, vp, i64],
         "pm_bfs": [vp, i32, vp, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_bfs_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_components": [vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
@@ -289,6 +290,26 @@ def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool 
     st = TraversalStats()
     _check(lib().pm_bfs(g.handle, int(start), pp, pd, mem, int(threshold), C.byref(st)))
     return (par, dep, st.as_dict()) if stats else (par, dep)
+
+
+def BFSMulti(sources, g: Graph, threshold: int = -1, device_out=None, stats: bool = False,
+             out=None):
+    """Depths from up to 64 sources in one traversal (uint64 source lanes per
+    vertex): a (k, n) int32 array, row l = BFS depths from sources[l]."""
+    src = np.ascontiguousarray(sources, np.int32)
+    k = len(src)
+    dep, pd, mem = _out(device_out, k * g.n, np.int32, None if out is None else out.reshape(-1))
+    if mem == PM_MEM_DEVICE:
+        import torch
+        src_t = torch.from_numpy(src).to(dep.device)
+        ps = C.c_void_p(src_t.data_ptr())
+        torch.cuda.synchronize()
+    else:
+        ps = src.ctypes.data_as(C.c_void_p)
+    st = TraversalStats()
+    _check(lib().pm_bfs_multi(g.handle, ps, k, pd, mem, int(threshold), C.byref(st)))
+    dep = dep.reshape(k, g.n)
+    return (dep, st.as_dict()) if stats else dep
 
 
 def Components(g: Graph, threshold: int = -1, device_out=None, stats: bool = False, out=None):

@@ -729,6 +729,12 @@ __global__ void k_vertex_map_bits(int32_t n, const uint32_t *__restrict__ bits, 
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
     if (test_bit(bits, (int)v)) f((int)v);
 }
+// vertexMap over a sparse frontier (the queue of a sparse round).
+template <class F>
+__global__ void k_vertex_map_queue(const int32_t *__restrict__ queue, int32_t size, F f) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size; i += stride) f(queue[i]);
+}
 // vertexMap over all vertices.
 template <class F>
 __global__ void k_vertex_map_all(int32_t n, F f) {
@@ -977,9 +983,17 @@ void edgeMapReduce(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_
   next.edges = (int64_t)h[0].edges;
 }
 
+// vertexMap (polymer.h:2340-2381): over the queue when the subset has one,
+// else over the bitmap.
 template <class F>
 void vertexMap(Engine &E, VertexSubset &s, F f) {
-  PM_LAUNCH((k_vertex_map_bits<F>), E.grid_for(s.n, 256, 16), 256, 0, E.stream, s.n, s.bits, f);
+  if (s.has_queue) {
+    if (s.size > 0)
+      PM_LAUNCH((k_vertex_map_queue<F>), E.grid_for(s.size, 256, 16), 256, 0, E.stream, s.queue,
+                (int32_t)s.size, f);
+  } else {
+    PM_LAUNCH((k_vertex_map_bits<F>), E.grid_for(s.n, 256, 16), 256, 0, E.stream, s.n, s.bits, f);
+  }
 }
 
 template <class F>

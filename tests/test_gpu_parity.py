@@ -180,6 +180,38 @@ def test_bfs_sparse_hubs(pm, oracle):
 
 # --------------------------------------------------------------------------
 @pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+@pytest.mark.parametrize("sym,k", [(True, 64), (False, 64), (True, 5)])
+def test_bfs_multi_matches_single_source(pm, oracle, threshold, sym, k):
+    og = oracle.rmat_graph(13, 16, symmetric=sym)
+    srcs = oracle.pick_sources(og, k, seed=0x5EED0015)
+    if k == 64:
+        srcs[7] = srcs[3]  # a repeated source must give identical rows
+    with dev_graph(pm, og, symmetric=sym) as g:
+        dep, st = pm.BFSMulti(srcs, g, threshold=threshold, stats=True)
+    reached, edges = 0, 0
+    deg = og.out_degree()
+    for l, s in enumerate(srcs):
+        ref, _ = oracle.bfs(og, int(s))
+        assert np.array_equal(dep[l], ref), "source %d (lane %d)" % (s, l)
+        reached += (ref >= 0).sum()
+        edges += deg[ref >= 0].sum()
+    assert st["reached"] == reached and st["edges_visited"] == edges
+
+
+def test_bfs_multi_device_out(pm, oracle):
+    import torch
+    og = oracle.rmat_graph(12, 16, symmetric=True)
+    srcs = oracle.pick_sources(og, 64)
+    with dev_graph(pm, og, symmetric=True) as g:
+        out = torch.empty((64, og.n), dtype=torch.int32, device="cuda")
+        dep = pm.BFSMulti(srcs, g, device_out=out, out=out)
+        assert dep.is_cuda
+        ref = pm.BFSMulti(srcs, g)
+    assert np.array_equal(dep.cpu().numpy(), ref)
+
+
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
 def test_components_exact(pm, oracle, threshold):
     for sym, scale in ((True, 13), (False, 12)):
         og = oracle.rmat_graph(scale, 8, symmetric=sym)
