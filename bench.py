@@ -283,9 +283,51 @@ def batched_block(pm, suite, reps=3):
         pm.BFS(s, A, device_out=suite.outA)
         ms_plain += A.timer_end()
     t = statistics.median(ms_multi)
-    return {"bfs64": {"ms": round(t, 3), "gteps": round(st["edges_visited"] / (t / 1e3) / 1e9, 2),
-                      "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
-                      "graph": "symmetrised R-MAT scale %d" % int(np.log2(A.n))}}
+    res = {"bfs64": {"ms": round(t, 3), "gteps": round(st["edges_visited"] / (t / 1e3) / 1e9, 2),
+                     "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
+                     "graph": "symmetrised R-MAT scale %d" % int(np.log2(A.n))}}
+    # personalised PageRank, 32 one-hot seeds, 20 iterations, n x 32 FP32
+    B = suite.B
+    offB, _ = B.csr()
+    seeds = suite._pick_sources(offB, 32, SEED_SRC + 200)
+    outp = suite.torch.empty((B.n, 32), dtype=suite.torch.float32, device=suite.dev)
+    pm.PersonalizedPageRank(B, seeds, 20, device_out=outp, out=outp)
+    B.timer_begin()
+    pm.PersonalizedPageRank(B, seeds, 20, device_out=outp, out=outp)
+    t_ppr = B.timer_end()
+    B.timer_begin()
+    pm.PageRank(B, 20, dtype=np.float32, device_out=suite.outB)
+    t_pr = B.timer_end()
+    nB, mB = B.n, B.m
+    res["ppr32"] = {"ms": round(t_ppr, 3), "gteps": round(32 * 20 * mB / (t_ppr / 1e3) / 1e9, 2),
+                    "hbm_gbs": round(20 * (132 * mB + 136 * nB) / (t_ppr / 1e3) / 1e9, 1),
+                    "plain_32_vectors_ms": round(32 * t_pr, 3),
+                    "speedup_vs_plain": round(32 * t_pr / t_ppr, 2),
+                    "plain": "32 x one FP32 PageRank run of 20 iterations (one vector per run)"}
+    # 256 Erdos-Renyi graphs, n log-uniform in [1k, 100k], avg degree 8, PageRank 20 it each
+    with pm.Graph.er_batch(256, 1000, 100000, 8) as G:
+        vb = G.parts()
+        outg = suite.torch.empty(G.n, dtype=suite.torch.float32, device=suite.dev)
+        pm.PageRankParts(G, 20, device_out=outg, out=outg)
+        G.timer_begin()
+        pm.PageRankParts(G, 20, device_out=outg, out=outg)
+        t_parts = G.timer_end()
+        off, idx = G.csr()
+        t_plain = 0.0
+        for i in range(len(vb) - 1):
+            a, b = int(vb[i]), int(vb[i + 1])
+            with pm.Graph.from_csr((off[a:b + 1] - off[a]).astype(np.int32),
+                                   (idx[off[a]:off[b]] - a).astype(np.int32)) as gi:
+                o = suite.torch.empty(b - a, dtype=suite.torch.float32, device=suite.dev)
+                gi.timer_begin()
+                pm.PageRank(gi, 20, dtype=np.float32, device_out=o, out=o)
+                t_plain += gi.timer_end()
+        res["er256_pagerank"] = {"ms": round(t_parts, 3), "n": int(G.n), "m": int(G.m),
+                                 "gteps": round(20 * G.m / (t_parts / 1e3) / 1e9, 2),
+                                 "plain_256_runs_ms": round(t_plain, 3),
+                                 "speedup_vs_plain": round(t_plain / t_parts, 2),
+                                 "launches": "one persistent launch (8-CTA clusters, work queue)"}
+    return res
 
 
 def ncu_traffic():

@@ -77,6 +77,23 @@ PM_API pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, i
 PM_API pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32_t flags,
                                int device, pm_graph **out);
 
+/* A batch of `count` independent directed Erdos-Renyi graphs stored as one
+ * disjoint union: part i has n_i vertices, log-uniform in [n_min, n_max], and
+ * n_i * avg_degree seeded draws (self loops, duplicates removed); vertex ids
+ * of part i start at parts[i] (pm_graph_get_parts).  The oracle's generator
+ * builds the same graph.  No reference counterpart (the reference runs one
+ * graph per process). */
+PM_API pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_max, int avg_degree,
+                                          uint64_t seed, int device, pm_graph **out);
+
+/* Declare g a disjoint union of count parts: part i owns vertices
+ * [vbase[i], vbase[i+1]) (host array of count+1 offsets, vbase[0] = 0,
+ * vbase[count] = n).  Rejected with PM_ERR_BAD_GRAPH if an edge crosses
+ * parts. */
+PM_API pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count);
+/* Part offsets (count+1 entries into vbase when vbase is not NULL). */
+PM_API pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count);
+
 PM_API pm_status pm_graph_destroy(pm_graph *g);
 
 /* n, m (directed stored edges) and max out-degree. */
@@ -157,6 +174,22 @@ PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32
  * resid (optional, iters doubles): sum |p_{t+1} - p_t| per iteration, FP64. */
 PM_API pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *ranks,
                       uint32_t mem, double *resid);
+
+/* PageRank (the semantics of pm_pagerank, FP32) on every part of a disjoint
+ * union independently, each with its own vertex count, all parts in ONE
+ * persistent kernel launch (thread-block clusters take parts from a work
+ * queue, largest first).  ranks: n floats in union vertex order. */
+PM_API pm_status pm_pagerank_parts(pm_graph *g, int iters, double damping, float *ranks,
+                                   uint32_t mem);
+
+/* Personalised PageRank for k <= 32 seeds in one SpMM-shaped pass per
+ * iteration.  No reference counterpart; built from PR_F's push p[s]/outdeg(s)
+ * (numa-PageRank.C:87-90) and PR_Vertex_F's damping (125-137) with the
+ * teleport going to the seed: x_0 = e_seed, x_{t+1}[d] = damping *
+ * sum_{s->d} x_t[s]/outdeg(s) + (1 - damping) * [d == seed] on every vertex.
+ * FP32 storage and sums.  out: n x k floats, row-major (out[v*k + j]). */
+PM_API pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, double damping,
+                        float *out, uint32_t mem);
 
 /* Weighted SpMV power iteration over the float weights.  Replaces
  * SPMV_main(WG, maxIter) (numa-SPMV.C:335) with SPMV_F (56-97): every

@@ -114,6 +114,46 @@ PMO_API int64_t pmo_rmat_graph(int scale, int ef, uint64_t seed, int symmetric,
   return m;
 }
 
+/* Batch of `count` directed Erdos-Renyi graphs as one disjoint union:      */
+/* graph i has n_i = floor(exp(ln n_min + u_i (ln n_max - ln n_min))) with   */
+/* u_i = (hash(seed, i) >> 11) * 2^-53 (log-uniform), and n_i * avg_degree   */
+/* draws (src, dst) = (h >> 32, h & 0xffffffff) mod n_i with h = hash(seed2, */
+/* running draw index), seed2 = seed ^ 0xE5E5E5E5; ids offset by vbase[i];   */
+/* self loops and duplicates removed, sorted.  vbase gets count+1 entries.   */
+PMO_API int64_t pmo_er_part_sizes(int count, int64_t n_min, int64_t n_max, uint64_t seed,
+                                  int64_t *vbase) {
+  vbase[0] = 0;
+  for (int i = 0; i < count; ++i) {
+    double u = (double)(pmo_hash(seed, (uint64_t)i) >> 11) * (1.0 / 9007199254740992.0);
+    int64_t ni = (int64_t)floor(exp(log((double)n_min) + u * (log((double)n_max) - log((double)n_min))));
+    if (ni < n_min) ni = n_min;
+    if (ni > n_max) ni = n_max;
+    vbase[i + 1] = vbase[i] + ni;
+  }
+  return vbase[count];
+}
+
+PMO_API int64_t pmo_er_batch(int count, int64_t n_min, int64_t n_max, int avg_degree, uint64_t seed,
+                             int64_t *vbase, int32_t *off, int32_t *idx) {
+  int64_t n = pmo_er_part_sizes(count, n_min, n_max, seed, vbase);
+  int64_t draws = n * avg_degree;
+  uint64_t *keys = (uint64_t *)malloc((size_t)(draws > 0 ? draws : 1) * sizeof(uint64_t));
+  uint64_t seed2 = seed ^ 0xE5E5E5E5ull;
+  int64_t k = 0;
+  for (int i = 0; i < count; ++i) {
+    int64_t ni = vbase[i + 1] - vbase[i];
+    for (int64_t j = 0; j < ni * avg_degree; ++j, ++k) {
+      uint64_t h = pmo_hash(seed2, (uint64_t)k);
+      uint64_t s = (uint64_t)vbase[i] + (h >> 32) % (uint64_t)ni;
+      uint64_t d = (uint64_t)vbase[i] + (h & 0xffffffffull) % (uint64_t)ni;
+      keys[k] = (s << 32) | d;
+    }
+  }
+  int64_t m = pmo_keys_to_csr(keys, draws, n, 0, off, idx);
+  free(keys);
+  return m;
+}
+
 /* Edge weight rules shared with the GPU generator (see DESIGN data layout). */
 PMO_API int32_t pmo_weight_int(uint64_t seed, uint32_t u, uint32_t v, int32_t wmax) {
   uint32_t a = u < v ? u : v, b = u < v ? v : u; /* symmetric: w(u,v) == w(v,u) */
@@ -227,6 +267,37 @@ PMO_API void pmo_pagerank(int64_t n, const int32_t *off, const int32_t *idx, int
   }
   memcpy(out, pc, (size_t)n * sizeof(double));
   free(pc); free(pn); free(F); free(Nx);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Personalised PageRank for k seeds (no reference; built from PR_F's push  */
+/* p[s]/outdeg(s), numa-PageRank.C:87-90, and PR_Vertex_F's damping,        */
+/* 125-137, with the teleport going to the seed):                           */
+/*   x_0 = e_seed,  x_{t+1}[d] = damping * sum_{s->d} x_t[s]/outdeg(s)      */
+/*                              + (1 - damping) * [d == seed]               */
+/* on every vertex, no dangling redistribution (as PR_F).  out: n x k,      */
+/* row-major (out[v*k + j] for seed j).                                      */
+/* ------------------------------------------------------------------------ */
+PMO_API void pmo_ppr(int64_t n, const int32_t *off, const int32_t *idx, const int32_t *seeds, int k,
+                     int iters, double damping, double *out) {
+  double *x = (double *)calloc((size_t)n * k, sizeof(double));
+  double *y = (double *)malloc((size_t)n * k * sizeof(double));
+  for (int j = 0; j < k; ++j) x[(int64_t)seeds[j] * k + j] = 1.0;
+  for (int it = 0; it < iters; ++it) {
+    memset(y, 0, (size_t)n * k * sizeof(double));
+    for (int64_t s = 0; s < n; ++s) {
+      int64_t deg = off[s + 1] - off[s];
+      for (int64_t e = off[s]; e < off[s + 1]; ++e) {
+        int32_t d = idx[e];
+        for (int j = 0; j < k; ++j) y[(int64_t)d * k + j] += x[s * k + j] / (double)deg;
+      }
+    }
+    for (int64_t i = 0; i < n * k; ++i) y[i] *= damping;
+    for (int j = 0; j < k; ++j) y[(int64_t)seeds[j] * k + j] += 1.0 - damping;
+    double *t = x; x = y; y = t;
+  }
+  memcpy(out, x, (size_t)n * k * sizeof(double));
+  free(x); free(y);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -66,6 +66,10 @@ def lib():
             "pmo_transpose": (None, [i64, i32p, i32p, i32p, i32p, C.c_void_p]),
             "pmo_pagerank": (None, [i64, i32p, i32p, C.c_int, C.c_double, f64p, C.c_void_p]),
             "pmo_spmv": (None, [i64, i32p, i32p, f64p, f64p, C.c_int, f64p]),
+            "pmo_ppr": (None, [i64, i32p, i32p, i32p, C.c_int, C.c_int, C.c_double, f64p]),
+            "pmo_er_part_sizes": (i64, [C.c_int, i64, i64, u64, np.ctypeslib.ndpointer(np.int64)]),
+            "pmo_er_batch": (i64, [C.c_int, i64, i64, C.c_int, u64, np.ctypeslib.ndpointer(np.int64),
+                                   i32p, i32p]),
             "pmo_bfs": (i64, [i64, i32p, i32p, i32, i32p, C.c_void_p]),
             "pmo_cc": (C.c_int, [i64, i32p, i32p, i32p]),
             "pmo_bellman_ford": (C.c_int, [i64, i32p, i32p, i32p, i32, i32p]),
@@ -116,6 +120,25 @@ def rmat_graph(scale: int, ef: int, seed: int = SEED_GRAPH, symmetric: bool = Fa
     idx = np.empty(max(cap, 1), np.int32)
     m = lib().pmo_rmat_graph(scale, ef, seed, int(symmetric), off, idx)
     return Graph(n, off, idx[:m].copy())
+
+
+def er_batch(count: int, n_min: int = 1000, n_max: int = 100000, avg_degree: int = 8,
+             seed: int = 0x5EED0006):
+    """Disjoint union of count seeded directed ER graphs: (Graph, vbase)."""
+    vbase = np.zeros(count + 1, np.int64)
+    n = lib().pmo_er_part_sizes(count, n_min, n_max, seed, vbase)
+    off = np.empty(n + 1, np.int32)
+    idx = np.empty(max(n * avg_degree, 1), np.int32)
+    m = lib().pmo_er_batch(count, n_min, n_max, avg_degree, seed, vbase, off, idx)
+    return Graph(int(n), off, idx[:m].copy()), vbase
+
+
+def subgraph(g: Graph, v0: int, v1: int) -> Graph:
+    """Induced subgraph on the contiguous range [v0, v1) of a graph whose
+    edges never leave that range (a part of a disjoint union)."""
+    off = (g.off[v0:v1 + 1] - g.off[v0]).astype(np.int32)
+    idx = (g.idx[g.off[v0]:g.off[v1]] - v0).astype(np.int32)
+    return Graph(v1 - v0, off, idx)
 
 
 def graph_from_edges(n: int, src, dst, symmetric: bool = False) -> Graph:
@@ -169,6 +192,14 @@ def pagerank(g: Graph, iters: int, damping: float = 0.85, with_resid: bool = Fal
     resid = np.zeros(max(iters, 1), np.float64)
     lib().pmo_pagerank(g.n, g.off, _idx(g), iters, damping, out, _ptr(resid))
     return (out, resid[:iters]) if with_resid else out
+
+
+def ppr(g: Graph, seeds, iters: int, damping: float = 0.85) -> np.ndarray:
+    """Personalised PageRank of len(seeds) seeds: (n, k) FP64."""
+    s = np.ascontiguousarray(seeds, np.int32)
+    out = np.empty(g.n * len(s), np.float64)
+    lib().pmo_ppr(g.n, g.off, _idx(g), s, len(s), iters, damping, out)
+    return out.reshape(g.n, len(s))
 
 
 def spmv(g: Graph, w, x0, iters: int) -> np.ndarray:

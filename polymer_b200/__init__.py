@@ -82,6 +82,11 @@ def lib():
         "pm_fill_uniform_f32": [vp, u64, C.c_int, vp, i64],
         "pm_bfs": [vp, i32, vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bfs_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_ppr": [vp, vp, C.c_int, C.c_int, C.c_double, vp, u32],
+        "pm_graph_create_er_batch": [C.c_int, i64, i64, C.c_int, u64, C.c_int, C.POINTER(vp)],
+        "pm_graph_set_parts": [vp, vp, C.c_int],
+        "pm_graph_get_parts": [vp, vp, C.POINTER(C.c_int)],
+        "pm_pagerank_parts": [vp, C.c_int, C.c_double, vp, u32],
         "pm_components": [vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
@@ -166,6 +171,28 @@ class Graph:
         _check(lib().pm_graph_create_rmat(scale, edge_factor, seed,
                                           PM_GRAPH_SYMMETRIC if symmetric else 0, device, C.byref(h)))
         return cls(h)
+
+    @classmethod
+    def er_batch(cls, count: int, n_min: int = 1000, n_max: int = 100000, avg_degree: int = 8,
+                 seed: int = 0x5EED0006, device: int = 0) -> "Graph":
+        """count independent directed Erdos-Renyi graphs as one disjoint union
+        (parts(): vertex offsets of the graphs)."""
+        h = C.c_void_p()
+        _check(lib().pm_graph_create_er_batch(count, n_min, n_max, avg_degree, seed, device,
+                                              C.byref(h)))
+        return cls(h)
+
+    def set_parts(self, vbase) -> None:
+        v = np.ascontiguousarray(vbase, np.int64)
+        _check(lib().pm_graph_set_parts(self._h, v.ctypes.data_as(C.c_void_p), len(v) - 1))
+
+    def parts(self) -> np.ndarray:
+        c = C.c_int()
+        _check(lib().pm_graph_get_parts(self._h, None, C.byref(c)))
+        v = np.zeros(c.value + 1, np.int64)
+        if c.value:
+            _check(lib().pm_graph_get_parts(self._h, v.ctypes.data_as(C.c_void_p), C.byref(c)))
+        return v
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -339,6 +366,31 @@ def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float6
                              PM_F64 if dt == np.float64 else PM_F32, pr, mem,
                              res.ctypes.data_as(C.c_void_p) if resid else None))
     return (ranks, res[:maxIter]) if resid else ranks
+
+
+def PageRankParts(g: Graph, maxIter: int = 20, damping: float = 0.85, device_out=None, out=None):
+    """PageRank of every part of a disjoint union (each with its own n), all
+    parts in one persistent launch: n float32 in union order."""
+    ranks, pr, mem = _out(device_out, g.n, np.float32, out)
+    _check(lib().pm_pagerank_parts(g.handle, int(maxIter), float(damping), pr, mem))
+    return ranks
+
+
+def PersonalizedPageRank(g: Graph, seeds, maxIter: int = 20, damping: float = 0.85,
+                         device_out=None, out=None):
+    """PPR for up to 32 seeds in one SpMM-shaped pass per iteration: (n, k) float32."""
+    s = np.ascontiguousarray(seeds, np.int32)
+    k = len(s)
+    res, po, mem = _out(device_out, g.n * k, np.float32, None if out is None else out.reshape(-1))
+    if mem == PM_MEM_DEVICE:
+        import torch
+        s_t = torch.from_numpy(s).to(res.device)
+        torch.cuda.synchronize()
+        ps = C.c_void_p(s_t.data_ptr())
+    else:
+        ps = s.ctypes.data_as(C.c_void_p)
+    _check(lib().pm_ppr(g.handle, ps, k, int(maxIter), float(damping), po, mem))
+    return res.reshape(g.n, k)
 
 
 def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False, out=None):

@@ -1,6 +1,10 @@
 // pm_batch.cu -- batched workloads on the engine: multi-source BFS with one
 // bit per source in a uint64 word per vertex.
+#include <cooperative_groups.h>
+
 #include "pm_graph.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pm {
 
@@ -135,6 +139,224 @@ void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, i
   s.reached = (int64_t)h[2].size;
   s.edges_visited = (int64_t)h[2].edges;
   if (st) *st = s;
+}
+
+// ===========================================================================
+// Personalised PageRank for up to 32 seeds in one SpMM-shaped pull per
+// iteration (PR_F's push p[s]/outdeg(s) and PR_Vertex_F's damping,
+// numa-PageRank.C:87-90, 125-137, applied to 32 vectors at once, teleport to
+// each vector's seed).  The contribution matrix C (n x 32 floats, row-major,
+// C[u][j] = x_j[u] / outdeg(u)) is gathered one 128-byte row per in-edge, a
+// full cache line; a warp owns a row and its lanes the 32 columns.  Rows
+// with more than kHeavyDeg in-edges are summed by chunk CTAs first.
+// ===========================================================================
+constexpr int kPprCols = 32;
+
+__device__ __forceinline__ float ppr_row_sum(const int32_t *__restrict__ idx, int64_t e0, int64_t e1,
+                                             const float *__restrict__ c, int lane, int stride_slices,
+                                             int first_slice) {
+  float acc = 0.f;
+  for (int64_t base = e0 + (int64_t)first_slice * 32; base < e1; base += (int64_t)stride_slices * 32) {
+    const int cnt = (int)min((int64_t)32, e1 - base);
+    const int my_s = lane < cnt ? __ldg(idx + base + lane) : 0;
+    for (int j0 = 0; j0 < cnt; j0 += 8) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int s = __shfl_sync(0xffffffffu, my_s, (j0 + u) & 31);
+        v[u] = (j0 + u < cnt) ? __ldg(c + (int64_t)s * kPprCols + lane) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc += v[u];
+    }
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(256) k_ppr_heavy(GraphView g, const float *__restrict__ c,
+                                                   float *__restrict__ partials) {
+  __shared__ float s_part[8][kPprCols];
+  const int ch = blockIdx.x;
+  if (ch >= g.in.nchunks) return;
+  const int lane = lane_id(), wid = threadIdx.x >> 5;
+  const int r = __ldg(g.in.hrow + ch);
+  const int k = ch - __ldg(g.in.hfirst + r);
+  const int64_t e0 = (int64_t)__ldg(g.in.off + r) + (int64_t)k * kChunkEdges;
+  const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.in.off + r + 1));
+  s_part[wid][lane] = ppr_row_sum(g.in.idx, e0, e1, c, lane, 8, wid);
+  __syncthreads();
+  if (wid == 0) {
+    float t = 0.f;
+    for (int w = 0; w < 8; ++w) t += s_part[w][lane];
+    partials[(int64_t)ch * kPprCols + lane] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ppr_pull(GraphView g, const float *__restrict__ c_cur,
+                                                  float *__restrict__ c_next, float *__restrict__ y_out,
+                                                  int k_out, const float *__restrict__ partials,
+                                                  const int32_t *__restrict__ seeds, float damping,
+                                                  Counters *ticket) {
+  const int lane = lane_id();
+  const int my_seed = lane < k_out ? __ldg(seeds + lane) : -1;
+  for (;;) {
+    int grp = 0;
+    if (lane == 0) grp = (int)atomicAdd(&ticket->aux, 1ull);
+    grp = __shfl_sync(0xffffffffu, grp, 0);
+    if (grp >= g.in.ngroups) break;
+    const int r0 = __ldg(g.in.gstart + grp), r1 = __ldg(g.in.gstart + grp + 1);
+    for (int r = r0; r < r1; ++r) {
+      const int64_t o0 = __ldg(g.in.off + r), o1 = __ldg(g.in.off + r + 1);
+      float acc;
+      if (o1 - o0 > kHeavyDeg) {
+        const int first = __ldg(g.in.hfirst + r);
+        const int nch = (int)((o1 - o0 + kChunkEdges - 1) / kChunkEdges);
+        acc = 0.f;
+        for (int q = 0; q < nch; ++q) acc += partials[(int64_t)(first + q) * kPprCols + lane];
+      } else {
+        acc = ppr_row_sum(g.in.idx, o0, o1, c_cur, lane, 1, 0);
+      }
+      const float y = damping * acc + (r == my_seed ? 1.0f - damping : 0.0f);
+      if (y_out && lane < k_out) y_out[(int64_t)r * k_out + lane] = y;
+      const int od = __ldg(g.out.off + r + 1) - __ldg(g.out.off + r);
+      c_next[(int64_t)r * kPprCols + lane] = od > 0 ? y / (float)od : 0.f;
+    }
+  }
+}
+
+__global__ void k_ppr_seed(const int32_t *seeds, int k, const int32_t *out_off, float *c, float *y0,
+                           int k_out) {
+  const int j = threadIdx.x;
+  if (j < k) {
+    const int v = seeds[j];
+    const int od = out_off[v + 1] - out_off[v];
+    c[(int64_t)v * kPprCols + j] = od > 0 ? 1.0f / (float)od : 0.f;
+    if (y0) y0[(int64_t)v * k_out + j] = 1.0f;
+  }
+}
+
+void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double damping, float *d_out) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  float *c0 = (float *)g->scratch_buf(0, (size_t)n * kPprCols * 4);
+  float *c1 = (float *)g->scratch_buf(1, (size_t)n * kPprCols * 4);
+  float *part = (float *)g->scratch_buf(2, (size_t)std::max(E.g.in.nchunks, 1) * kPprCols * 4);
+  PM_CUDA(cudaMemsetAsync(c0, 0, (size_t)n * kPprCols * 4, E.stream));
+  if (iters == 0) PM_CUDA(cudaMemsetAsync(d_out, 0, (size_t)n * k * 4, E.stream));
+  PM_LAUNCH(k_ppr_seed, 1, 32, 0, E.stream, d_seeds, k, E.g.out.off, c0, iters == 0 ? d_out : nullptr, k);
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppr_pull, 256, 0));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)E.g.in.ngroups + 7) / 8,
+                                                               (int64_t)E.num_sms * per_sm));
+  for (int it = 0; it < iters; ++it) {
+    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+    E.prof.begin("ppr", E.stream);
+    if (E.g.in.nchunks > 0)
+      PM_LAUNCH(k_ppr_heavy, E.g.in.nchunks, 256, 0, E.stream, E.g, c0, part);
+    PM_LAUNCH(k_ppr_pull, grid, 256, 0, E.stream, E.g, c0, c1, it == iters - 1 ? d_out : nullptr, k,
+              part, d_seeds, (float)damping, E.d_cnt);
+    E.prof.end(E.stream);
+    std::swap(c0, c1);
+  }
+}
+
+// ===========================================================================
+// Many independent graphs (the parts of a disjoint union) each running
+// PageRank with Polymer's semantics (PR_F / PR_Vertex_F / PR_Vertex_Reset,
+// numa-PageRank.C:64-148, n = the part's own vertex count), all in ONE
+// persistent launch.  Thread-block clusters of kPartCluster CTAs take parts
+// from a work queue, largest first; the CTAs of a cluster split the part's
+// vertices and separate the phases of an iteration with the cluster barrier
+// (barrier.cluster, a hardware barrier: no flag is polled).  One thread per
+// vertex sums its in-edges; the frontier rides in the contribution sign as in
+// run_pagerank.
+// ===========================================================================
+constexpr int kPartCluster = 8;
+constexpr int kPartThreads = 512;
+
+__global__ void __cluster_dims__(kPartCluster, 1, 1) __launch_bounds__(kPartThreads)
+    k_pagerank_parts(GraphView g, const int64_t *__restrict__ vbase, const int32_t *__restrict__ order,
+                     int count, int iters, float damping, float *pc, float *pn, float *c0, float *c1,
+                     float *out, Counters *queue) {
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ int s_part;
+  const int rank = (int)cluster.block_rank();
+  const int64_t stride = (int64_t)kPartCluster * kPartThreads;
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) s_part = (int)atomicAdd(&queue->aux, 1ull);
+    cluster.sync();
+    const int part = *cluster.map_shared_rank(&s_part, 0);
+    cluster.sync();  // every CTA has read the ticket before the next one is drawn
+    if (part >= count) break;
+    const int p = __ldg(order + part);
+    const int64_t v0 = __ldg(vbase + p), v1 = __ldg(vbase + p + 1);
+    const float p0 = 1.0f / (float)(v1 - v0);
+    const float added = (1.0f - damping) * p0;
+    const int64_t first = v0 + (int64_t)rank * kPartThreads + threadIdx.x;
+    for (int64_t v = first; v < v1; v += stride) {
+      const int deg = __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+      pc[v] = p0;
+      pn[v] = 0.0f;
+      c0[v] = deg > 0 ? p0 / (float)deg : 0.0f;
+    }
+    cluster.sync();
+    float *A = pc, *B = pn, *cc = c0, *cn = c1;
+    for (int it = 0; it < iters; ++it) {
+      for (int64_t v = first; v < v1; v += stride) {
+        const int e0 = __ldg(g.in.off + v), e1 = __ldg(g.in.off + v + 1);
+        float acc = -0.0f;
+        int e = e0;
+        for (; e + 3 < e1; e += 4) {
+          const int s0 = __ldg(g.in.idx + e), s1 = __ldg(g.in.idx + e + 1);
+          const int s2 = __ldg(g.in.idx + e + 2), s3 = __ldg(g.in.idx + e + 3);
+          acc += (cc[s0] + cc[s1]) + (cc[s2] + cc[s3]);
+        }
+        for (; e < e1; ++e) acc += cc[__ldg(g.in.idx + e)];
+        const bool in_f = !signbit(cc[v]);
+        const bool hit = !signbit(acc);
+        float nb = B[v] + acc;
+        if (in_f) {
+          nb = damping * nb + added;
+          A[v] = 0.0f;
+        }
+        B[v] = nb;
+        const int deg = __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+        cn[v] = hit ? (deg > 0 ? nb / (float)deg : 0.0f) : -0.0f;
+      }
+      cluster.sync();
+      float *t = A; A = B; B = t;
+      t = cc; cc = cn; cn = t;
+    }
+    for (int64_t v = first; v < v1; v += stride) out[v] = A[v];
+    cluster.sync();
+  }
+}
+
+void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  const int count = (int)g->parts.size() - 1;
+  float *pc = (float *)g->scratch_buf(0, (size_t)n * 4);
+  float *pn = (float *)g->scratch_buf(1, (size_t)n * 4);
+  float *c0 = (float *)g->scratch_buf(2, (size_t)n * 4);
+  float *c1 = (float *)g->scratch_buf(3, (size_t)n * 4);
+  static int clusters = 0;
+  if (clusters == 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kPartCluster * 64);
+    cfg.blockDim = dim3(kPartThreads);
+    PM_CUDA(cudaOccupancyMaxActiveClusters(&clusters, (void *)k_pagerank_parts, &cfg));
+    if (clusters < 1) clusters = 1;
+  }
+  const int grid = kPartCluster * std::max(1, std::min(clusters, count));
+  PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+  E.prof.begin("pagerank_parts", E.stream);
+  PM_LAUNCH(k_pagerank_parts, grid, kPartThreads, 0, E.stream, E.g, g->parts_vbase.as<int64_t>(),
+            g->parts_order.as<int32_t>(), count, iters, (float)damping, pc, pn, c0, c1, d_out, E.d_cnt);
+  E.prof.end(E.stream);
 }
 
 }  // namespace pm

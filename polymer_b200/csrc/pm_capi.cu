@@ -24,6 +24,12 @@ void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_n
 void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
 void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, int64_t threshold,
                pm_traversal_stats *st);
+void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double damping, float *d_out);
+void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out);
+void generate_er_batch(pm_graph *g, int count, int64_t n_min, int64_t n_max, int avg_degree,
+                       uint64_t seed);
+void check_parts(pm_graph *g, const std::vector<int64_t> &vbase);
+void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
 }  // namespace pm
 
 using namespace pm;
@@ -152,6 +158,62 @@ pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32
       throw;
     }
     *out = g;
+  });
+}
+
+pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_max, int avg_degree,
+                                   uint64_t seed, int device, pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(count >= 1 && count <= 1 << 20, "count must be in [1, 2^20]");
+    need(n_min >= 2 && n_max >= n_min && n_max < (1ll << 30), "need 2 <= n_min <= n_max < 2^30");
+    need(avg_degree >= 1 && avg_degree <= 64, "avg_degree must be in [1, 64]");
+    pm_graph *g = new_graph(device, false);
+    try {
+      generate_er_batch(g, count, n_min, n_max, avg_degree, seed);
+      finish_graph(g);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count) {
+  return guard([&] {
+    enter(g);
+    need(vbase != nullptr && count >= 1, "need count >= 1 part offsets");
+    std::vector<int64_t> v(vbase, vbase + count + 1);
+    check_parts(g, v);
+    set_parts(g, v);
+  });
+}
+
+pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count) {
+  return guard([&] {
+    need(g != nullptr, "null graph handle");
+    const int c = g->parts.empty() ? 0 : (int)g->parts.size() - 1;
+    if (count) *count = c;
+    if (vbase && c) memcpy(vbase, g->parts.data(), (size_t)(c + 1) * 8);
+  });
+}
+
+pm_status pm_pagerank_parts(pm_graph *g, int iters, double damping, float *ranks, uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(ranks != nullptr, "null ranks");
+    need(iters >= 0, "iters must be >= 0");
+    need(!g->parts.empty(), "graph has no parts (pm_graph_set_parts)");
+    need(!g->has_self_loops,
+         "PageRank needs a graph without self loops (create it with PM_GRAPH_SKIP_SELF_LOOPS)");
+    const size_t bytes = (size_t)g->n * 4;
+    float *dr = mem == PM_MEM_DEVICE ? ranks : (float *)g->scratch_buf(kSlotOut0, bytes);
+    run_pagerank_parts(g, iters, damping, dr);
+    if (mem == PM_MEM_HOST) from_device(g, ranks, dr, bytes, mem);
+    finish(g);
   });
 }
 
@@ -337,6 +399,32 @@ pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *r
       run_pagerank<float>(g, iters, damping, (float *)dr, dres);
     if (mem == PM_MEM_HOST) from_device(g, ranks, dr, bytes, mem);
     if (resid && iters > 0) from_device(g, resid, dres, (size_t)iters * 8, PM_MEM_HOST);
+    finish(g);
+  });
+}
+
+pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, double damping, float *out,
+                 uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(seeds != nullptr && out != nullptr, "null seeds/out");
+    need(k >= 1 && k <= 32, "k must be in [1, 32]");
+    need(iters >= 0, "iters must be >= 0");
+    need(!g->has_self_loops,
+         "PageRank needs a graph without self loops (create it with PM_GRAPH_SKIP_SELF_LOOPS)");
+    int32_t hs[32];
+    if (mem == PM_MEM_DEVICE)
+      PM_CUDA(cudaMemcpy(hs, seeds, (size_t)k * 4, cudaMemcpyDeviceToHost));
+    else
+      memcpy(hs, seeds, (size_t)k * 4);
+    for (int j = 0; j < k; ++j) need(hs[j] >= 0 && hs[j] < g->n, "seed out of range");
+    int32_t *ds = (int32_t *)g->scratch_buf(kSlotIn0, 32 * 4);
+    PM_CUDA(cudaMemcpyAsync(ds, hs, (size_t)k * 4, cudaMemcpyHostToDevice, g->E.stream));
+    const size_t bytes = (size_t)g->n * k * 4;
+    float *dout = mem == PM_MEM_DEVICE ? out : (float *)g->scratch_buf(kSlotOut0, bytes);
+    run_ppr(g, ds, k, iters, damping, dout);
+    if (mem == PM_MEM_HOST) from_device(g, out, dout, bytes, mem);
     finish(g);
   });
 }

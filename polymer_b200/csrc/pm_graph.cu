@@ -4,6 +4,8 @@
 // CUB (library code) as plain primitives.
 #include <cub/cub.cuh>
 
+#include <cmath>
+
 #include "pm_graph.cuh"
 
 namespace pm {
@@ -362,19 +364,16 @@ void ingest_csr(pm_graph *g, bool skip_self_loops) {
 }
 
 // Seeded R-MAT straight into the device CSR.
-void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed) {
+// Sorts the (src << 32 | dst) keys in a (self loops replaced by a sentinel
+// >= n << 32 below 2^(end_bit)), drops duplicates and the sentinel, and
+// builds g's CSR.
+static void keys_to_csr(pm_graph *g, DevBuf &a, DevBuf &b, int64_t nkeys, int64_t n, int end_bit) {
   cudaStream_t st = g->E.stream;
-  const int64_t n = (int64_t)1 << scale;
-  const int64_t draws = n * ef;
-  const int64_t nkeys = draws * (g->symmetric ? 2 : 1);
-  DevBuf a((size_t)nkeys * 8), b((size_t)nkeys * 8);
-  PM_LAUNCH(k_rmat_keys, grid1d(draws), 256, 0, st, scale, seed, draws, (int)g->symmetric,
-            a.as<uint64_t>());
   cub::DoubleBuffer<uint64_t> db(a.as<uint64_t>(), b.as<uint64_t>());
   size_t tmp = 0;
-  PM_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, db, (int)nkeys, 0, 33 + scale, st));
+  PM_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, db, (int)nkeys, 0, end_bit, st));
   DevBuf tb(tmp);
-  PM_CUDA(cub::DeviceRadixSort::SortKeys(tb.p, tmp, db, (int)nkeys, 0, 33 + scale, st));
+  PM_CUDA(cub::DeviceRadixSort::SortKeys(tb.p, tmp, db, (int)nkeys, 0, end_bit, st));
   uint64_t *sorted = db.Current();
   uint64_t *uniq = db.Alternate();
   DevBuf nsel(8);
@@ -397,6 +396,118 @@ void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed) {
   if (m) PM_LAUNCH(k_keys_to_csr_idx, grid1d(m), 256, 0, st, uniq, m, g->out.idx.as<int32_t>());
   PM_LAUNCH(k_keys_offsets, grid1d(n + 1), 256, 0, st, uniq, m, n, g->out.off.as<int32_t>());
   PM_CUDA(cudaStreamSynchronize(st));
+}
+
+void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed) {
+  const int64_t n = (int64_t)1 << scale;
+  const int64_t draws = n * ef;
+  const int64_t nkeys = draws * (g->symmetric ? 2 : 1);
+  DevBuf a((size_t)nkeys * 8), b((size_t)nkeys * 8);
+  PM_LAUNCH(k_rmat_keys, grid1d(draws), 256, 0, g->E.stream, scale, seed, draws, (int)g->symmetric,
+            a.as<uint64_t>());
+  keys_to_csr(g, a, b, nkeys, n, 33 + scale);
+}
+
+// Erdos-Renyi batch: the rule of the oracle's pmo_er_batch.
+__global__ void k_er_keys(const int64_t *vbase, const int64_t *dbase, int count, int64_t draws,
+                          uint64_t seed2, uint64_t sentinel, uint64_t *keys) {
+  GRID_STRIDE(k, draws) {
+    int lo = 0, hi = count - 1;  // graph of draw k: last i with dbase[i] <= k
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (dbase[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const uint64_t ni = (uint64_t)(vbase[lo + 1] - vbase[lo]);
+    const uint64_t h = hash64(seed2, (uint64_t)k);
+    const uint64_t s = (uint64_t)vbase[lo] + (h >> 32) % ni;
+    const uint64_t d = (uint64_t)vbase[lo] + (h & 0xffffffffull) % ni;
+    keys[k] = s == d ? sentinel : ((s << 32) | d);
+  }
+}
+
+// Part sizes of the ER batch (host; the oracle's pmo_er_part_sizes).
+std::vector<int64_t> er_part_sizes(int count, int64_t n_min, int64_t n_max, uint64_t seed) {
+  std::vector<int64_t> vbase(count + 1, 0);
+  for (int i = 0; i < count; ++i) {
+    const double u = (double)(hash64(seed, (uint64_t)i) >> 11) * (1.0 / 9007199254740992.0);
+    int64_t ni = (int64_t)std::floor(std::exp(std::log((double)n_min) +
+                                              u * (std::log((double)n_max) - std::log((double)n_min))));
+    ni = std::min(std::max(ni, n_min), n_max);
+    vbase[i + 1] = vbase[i] + ni;
+  }
+  return vbase;
+}
+
+void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
+
+void generate_er_batch(pm_graph *g, int count, int64_t n_min, int64_t n_max, int avg_degree,
+                       uint64_t seed) {
+  std::vector<int64_t> vbase = er_part_sizes(count, n_min, n_max, seed);
+  const int64_t n = vbase[count];
+  std::vector<int64_t> dbase(count + 1);
+  for (int i = 0; i <= count; ++i) dbase[i] = vbase[i] * avg_degree;
+  const int64_t draws = dbase[count];
+  if (n >= (1ll << 31) - 1 || draws >= (1ll << 31) - 1)
+    fail(PM_ERR_INVALID_ARG, "batch exceeds int32 ids or edge offsets");
+  int bits = 1;
+  while ((1ll << bits) <= n) ++bits;
+  DevBuf dv((size_t)(count + 1) * 8), dd((size_t)(count + 1) * 8);
+  PM_CUDA(cudaMemcpyAsync(dv.p, vbase.data(), (count + 1) * 8, cudaMemcpyHostToDevice, g->E.stream));
+  PM_CUDA(cudaMemcpyAsync(dd.p, dbase.data(), (count + 1) * 8, cudaMemcpyHostToDevice, g->E.stream));
+  DevBuf a((size_t)std::max<int64_t>(draws, 1) * 8), b((size_t)std::max<int64_t>(draws, 1) * 8);
+  PM_LAUNCH(k_er_keys, grid1d(draws), 256, 0, g->E.stream, dv.as<int64_t>(), dd.as<int64_t>(), count,
+            draws, seed ^ 0xE5E5E5E5ull, (uint64_t)1 << (32 + bits), a.as<uint64_t>());
+  keys_to_csr(g, a, b, draws, n, 33 + bits);
+  set_parts(g, vbase);
+}
+
+// err |= 1 when an edge leaves its source's part.
+__global__ void k_check_parts(const int32_t *off, const int32_t *idx, int64_t n, const int64_t *vbase,
+                              int count, unsigned int *err) {
+  GRID_STRIDE(v, n) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (vbase[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    const int64_t a = vbase[lo], b = vbase[lo + 1];
+    for (int32_t e = off[v]; e < off[v + 1]; ++e)
+      if (idx[e] < a || idx[e] >= b) atomicOr(err, 1u);
+  }
+}
+
+void check_parts(pm_graph *g, const std::vector<int64_t> &vbase) {
+  const int count = (int)vbase.size() - 1;
+  if (count < 1 || vbase[0] != 0 || vbase[count] != g->n)
+    fail(PM_ERR_INVALID_ARG, "parts must start at 0 and end at n");
+  for (int i = 0; i < count; ++i)
+    if (vbase[i + 1] <= vbase[i]) fail(PM_ERR_INVALID_ARG, "parts must be non-empty and increasing");
+  DevBuf dv((size_t)(count + 1) * 8), err(4);
+  PM_CUDA(cudaMemcpyAsync(dv.p, vbase.data(), (count + 1) * 8, cudaMemcpyHostToDevice, g->E.stream));
+  PM_CUDA(cudaMemsetAsync(err.p, 0, 4, g->E.stream));
+  PM_LAUNCH(k_check_parts, grid1d(g->n), 256, 0, g->E.stream, g->out.off.as<int32_t>(),
+            g->out.idx.as<int32_t>(), g->n, dv.as<int64_t>(), count, err.as<unsigned int>());
+  unsigned int h = 0;
+  PM_CUDA(cudaMemcpyAsync(&h, err.p, 4, cudaMemcpyDeviceToHost, g->E.stream));
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+  if (h) fail(PM_ERR_BAD_GRAPH, "an edge crosses two parts");
+}
+
+// Part boundaries and the largest-first processing order.
+void set_parts(pm_graph *g, const std::vector<int64_t> &vbase) {
+  const int count = (int)vbase.size() - 1;
+  std::vector<int32_t> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return vbase[a + 1] - vbase[a] > vbase[b + 1] - vbase[b];
+  });
+  g->parts_vbase.alloc((size_t)(count + 1) * 8);
+  g->parts_order.alloc((size_t)std::max(count, 1) * 4);
+  PM_CUDA(cudaMemcpyAsync(g->parts_vbase.p, vbase.data(), (count + 1) * 8, cudaMemcpyHostToDevice,
+                          g->E.stream));
+  PM_CUDA(cudaMemcpyAsync(g->parts_order.p, order.data(), count * 4, cudaMemcpyHostToDevice, g->E.stream));
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+  g->parts = vbase;
 }
 
 void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float) {

@@ -76,6 +76,10 @@ struct pm_graph {
   pm::Counters *h_cnt = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<pm::DevBuf> scratch;  // per-call workspaces kept across calls
+  // disjoint parts (a batch of independent graphs): vertex ranges and the
+  // largest-first order in which persistent kernels take them
+  std::vector<int64_t> parts;       // count+1 vertex offsets (host copy); empty if none
+  pm::DevBuf parts_vbase, parts_order;
 
   pm::VertexSubset subset(int k) {
     pm::VertexSubset s;

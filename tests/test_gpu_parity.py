@@ -271,6 +271,63 @@ def test_spmv_f32_rel_l1(pm, oracle):
 
 
 # --------------------------------------------------------------------------
+@pytest.mark.parametrize("k", [32, 3])
+def test_ppr_matches_oracle(pm, oracle, k):
+    og = oracle.rmat_graph(14, 16)
+    seeds = oracle.pick_sources(og, k, seed=0x5EED0025)
+    ref = oracle.ppr(og, seeds, 20)
+    with dev_graph(pm, og) as g:
+        out = pm.PersonalizedPageRank(g, seeds, 20)
+    assert out.shape == (og.n, k)
+    for j in range(k):
+        assert rel_l1(out[:, j], ref[:, j]) < RL1_F32, j
+    with dev_graph(pm, og) as g:
+        assert np.array_equal(pm.PersonalizedPageRank(g, seeds, 0)[seeds, np.arange(k)], np.ones(k))
+
+
+def test_ppr_heavy_rows(pm, oracle):
+    # star into vertex 0 from 5000 sources (a heavy CSC row) plus a chain
+    n = 6000
+    src = np.concatenate([np.arange(1, 5001), np.arange(5001, 5999)])
+    dst = np.concatenate([np.zeros(5000, np.int64), np.arange(5002, 6000)])
+    og = oracle.graph_from_edges(n, np.concatenate([src, [0]]), np.concatenate([dst, [5001]]))
+    seeds = [1, 2, 5001, 0]
+    ref = oracle.ppr(og, seeds, 15)
+    with dev_graph(pm, og) as g:
+        out = pm.PersonalizedPageRank(g, seeds, 15)
+    for j in range(len(seeds)):
+        assert rel_l1(out[:, j], ref[:, j]) < RL1_F32
+
+
+def test_er_batch_generator_and_parts_pagerank(pm, oracle):
+    og, vbase = oracle.er_batch(24, 100, 3000, 8, seed=77)
+    with pm.Graph.er_batch(24, 100, 3000, 8, seed=77) as g:
+        off, idx = g.csr()
+        assert np.array_equal(g.parts(), vbase)
+        assert np.array_equal(off, og.off) and np.array_equal(idx, og.idx)
+        ranks = pm.PageRankParts(g, 20)
+    for i in range(24):
+        sub = oracle.subgraph(og, int(vbase[i]), int(vbase[i + 1]))
+        ref = oracle.pagerank(sub, 20)
+        assert rel_l1(ranks[vbase[i]:vbase[i + 1]], ref) < RL1_F32, i
+
+
+def test_parts_from_user_graph(pm, oracle):
+    # two R-MAT graphs side by side as one union, parts declared by the caller
+    a = oracle.rmat_graph(10, 8)
+    b = oracle.rmat_graph(11, 8, seed=5)
+    off = np.concatenate([a.off[:-1], b.off + a.m]).astype(np.int32)
+    idx = np.concatenate([a.idx, b.idx + a.n]).astype(np.int32)
+    with pm.Graph.from_csr(off, idx) as g:
+        g.set_parts([0, a.n, a.n + b.n])
+        ranks = pm.PageRankParts(g, 12)
+        with pytest.raises(pm.PolymerError):
+            g.set_parts([0, 100, a.n + b.n])  # edges cross this split
+    assert rel_l1(ranks[:a.n], oracle.pagerank(a, 12)) < RL1_F32
+    assert rel_l1(ranks[a.n:], oracle.pagerank(b, 12)) < RL1_F32
+
+
+# --------------------------------------------------------------------------
 def test_bp_matches_oracle(pm, oracle):
     og = oracle.rmat_graph(14, 16)
     prior = oracle.uniform_open(2 * og.n).reshape(og.n, 2)

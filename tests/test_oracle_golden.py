@@ -110,6 +110,28 @@ def test_bp_restatement_small(oracle):
     assert np.allclose(out[0], [0, 0])
 
 
+def test_er_batch_generator(oracle):
+    g, vbase = oracle.er_batch(40, 50, 5000, 8, seed=3)
+    sizes = np.diff(vbase)
+    assert sizes.min() >= 50 and sizes.max() <= 5000 and len(sizes) == 40
+    src = np.repeat(np.arange(g.n), np.diff(g.off))
+    part = np.searchsorted(vbase, src, side="right") - 1
+    assert np.all(g.idx >= vbase[part]) and np.all(g.idx < vbase[part + 1]), "edges stay in their part"
+    assert np.all(src != g.idx)
+    assert abs(g.m / g.n - 8) < 0.5
+
+
+def test_ppr_restatement(oracle):
+    g = oracle.rmat_graph(9, 8)
+    seeds = oracle.pick_sources(g, 4)
+    x = oracle.ppr(g, seeds, 30)
+    # fixed point check: x = d P^T x + (1-d) e_seed (30 iterations ~ 0.85^30)
+    for j, s in enumerate(seeds):
+        y = oracle.ppr(g, [s], 31)[:, 0]
+        assert np.abs(x[:, j] - y).sum() < 0.05
+        assert x[s, j] >= 0.15
+
+
 def test_depths_from_parents_rejects_cycles(oracle):
     with pytest.raises(ValueError):
         oracle.bfs_depths_from_parents(np.array([0, 2, 1], np.int32), 0)
