@@ -330,6 +330,53 @@ def batched_block(pm, suite, reps=3):
     return res
 
 
+def adjoint_block(pm, torch, dev, reps=3):
+    """weighted PageRank on directed R-MAT scale 20 with
+    lognormal(0,1) weights normalised per source row, damping 0.85, solved to
+    1e-6 relative L1; loss = sum of the ranks of 1024 seeded targets; adjoint
+    (transposed iteration + per-edge gradient) vs forward solve, and the
+    weighted SpMV backward vs one forward SpMV, device time."""
+    with pm.Graph.rmat(20, 16, seed=SEED_GRAPH) as G:
+        G.gen_weights_lognormal(0x5EED0007)
+        n, m = G.n, G.m
+        tgt = []
+        j = 0
+        while len(tgt) < 1024:
+            v = Suite._hash(0x5EED0008, j) % n
+            j += 1
+            if v not in tgt:
+                tgt.append(v)
+        gp = torch.zeros(n, dtype=torch.float32, device=dev)
+        gp[torch.tensor(tgt, device=dev)] = 1.0
+        p = torch.empty(n, dtype=torch.float32, device=dev)
+        dw = torch.empty(m, dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        fwd, adj, it_f, it_a = [], [], 0, 0
+        for _ in range(reps + 1):
+            G.timer_begin()
+            _, it_f, _ = pm.WeightedPageRank(G, 0.85, 1e-6, 1000, device_out=p, out=p)
+            fwd.append(G.timer_end())
+            G.timer_begin()
+            _, it_a = pm.PageRankAdjoint(G, p, gp, 0.85, 1e-6, 1000, out=dw)
+            adj.append(G.timer_end())
+        x = pm.uniform_f32(G, n, SEED_X)
+        G.timer_begin()
+        for _ in range(10):
+            pm.SPMV(G, x, 1)
+        t_spmv = G.timer_end() / 10
+        G.timer_begin()
+        for _ in range(10):
+            pm.SpMVBackward(G, x, gp)
+        t_spmvb = G.timer_end() / 10
+        tf, ta = statistics.median(fwd[1:]), statistics.median(adj[1:])
+        return {"graph": "directed R-MAT scale 20 (n=%d, m=%d), lognormal weights" % (n, m),
+                "forward_ms": round(tf, 3), "forward_iters": it_f, "adjoint_ms": round(ta, 3),
+                "adjoint_iters": it_a, "adjoint_over_forward": round(ta / tf, 3),
+                "spmv_ms": round(t_spmv, 3), "spmv_backward_ms": round(t_spmvb, 3),
+                "spmv_backward_over_forward": round(t_spmvb / t_spmv, 3),
+                "tolerance": "relative L1 residual 1e-6, FP64 sums"}
+
+
 def ncu_traffic():
     """DRAM bytes per PageRank pass from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "pagerank_pull_rmat24.md")
@@ -583,6 +630,7 @@ def main():
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     if not args.no_batched:
         line["batched"] = batched_block(pm, suite)
+        line["adjoint"] = adjoint_block(pm, torch, suite.dev)
     if not args.no_e2e:
         line["e2e"] = e2e_run(pm, suite, args.e2e_steps)
     if dist:

@@ -199,6 +199,37 @@ PM_API pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, dou
 PM_API pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem,
                   double *norm1);
 
+/* ---- Differentiation (no reference counterpart; weighted forms of SPMV_F,
+ * numa-SPMV.C:72-81, with PR_Vertex_F's damping, numa-PageRank.C:125-137).
+ * W = the float weights of pm_graph_set_weights_f32, per CSR edge, and
+ * (A_W^T x)[v] = sum_{e = s->v} W_e x[s].  Fixed points iterate until
+ * sum|x_{t+1} - x_t| <= tol * sum|x_{t+1}| (FP64 sums on the device) or
+ * max_iters; *iters / *resid report the passes and the last relative change.
+ * All float arrays live in mem's space. */
+
+/* Weighted PageRank p = damping * A_W^T p + (1 - damping)/n from p = 1/n. */
+PM_API pm_status pm_weighted_pagerank(pm_graph *g, double damping, double tol, int max_iters,
+                                      float *p, uint32_t mem, int *iters, double *resid);
+
+/* Adjoint of the weighted PageRank fixed point for a cotangent grad_p
+ * (dL/dp, n floats) at the solution p: lambda = damping * A_W lambda +
+ * grad_p by the transposed iteration (a pull over the CSR), then
+ * dw[e] = dL/dW_e = damping * lambda[v] * p[s] for every CSR edge e = s->v
+ * (m floats).  lambda (n floats) may be NULL. */
+PM_API pm_status pm_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters,
+                                     const float *p, const float *grad_p, float *dw, float *lambda,
+                                     uint32_t mem, int *iters, double *resid);
+
+/* Backward of one weighted SpMV y = A_W^T x for a cotangent grad_y:
+ * dx = A_W grad_y (a pull over the CSR, n floats), dw[e] = grad_y[v] * x[s]
+ * (m floats).  Either output may be NULL. */
+PM_API pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, float *dx,
+                                  float *dw, uint32_t mem);
+
+/* Lognormal(0, 1) weights normalised per source row, generated on the
+ * device and set as the graph's float weights. */
+PM_API pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed);
+
 /* Two-state belief propagation.  Replaces BeliefPropagation(G, maxIter)
  * (numa-BP.C:528) with BP_F / BP_Vertex_Reset (89-140) and
  * edgeMapDenseBPNoRep (179-230): for every out-edge s->d of the frontier,

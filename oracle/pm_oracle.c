@@ -301,6 +301,99 @@ PMO_API void pmo_ppr(int64_t n, const int32_t *off, const int32_t *idx, const in
 }
 
 /* ------------------------------------------------------------------------ */
+/* Weighted PageRank and its adjoint (no reference counterpart; the          */
+/* weighted push of SPMV_F, numa-SPMV.C:72-81, with PR_Vertex_F's damping,   */
+/* numa-PageRank.C:125-137, on every vertex):                                */
+/*   p = damping * A_W^T p + (1 - damping)/n,  (A_W^T p)[v] = sum_{e=s->v}   */
+/*   W_e p[s],  p_0 = 1/n, iterated until sum|p_{t+1} - p_t| <= tol*sum|p|.   */
+/* For a cotangent g (dL/dp) the adjoint solves lambda = damping * A_W       */
+/* lambda + g, (A_W lambda)[s] = sum_{e=s->v} W_e lambda[v], by the same     */
+/* iteration from lambda_0 = g, and dL/dW_e = damping * lambda[v] * p[s].    */
+/* Weights are per CSR edge; returns the number of iterations.               */
+/* ------------------------------------------------------------------------ */
+PMO_API int pmo_weighted_pagerank(int64_t n, const int32_t *off, const int32_t *idx, const double *w,
+                                  double damping, double tol, int max_iters, double *p) {
+  double *q = (double *)malloc((size_t)n * sizeof(double));
+  for (int64_t i = 0; i < n; ++i) p[i] = 1.0 / (double)n;
+  int it = 0;
+  while (it < max_iters) {
+    for (int64_t i = 0; i < n; ++i) q[i] = 0.0;
+    for (int64_t s = 0; s < n; ++s)
+      for (int64_t e = off[s]; e < off[s + 1]; ++e) q[idx[e]] += w[e] * p[s];
+    double r = 0.0, tot = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      q[i] = damping * q[i] + (1.0 - damping) / (double)n;
+      r += fabs(q[i] - p[i]);
+      tot += fabs(q[i]);
+    }
+    memcpy(p, q, (size_t)n * sizeof(double));
+    ++it;
+    if (r <= tol * tot) break;
+  }
+  free(q);
+  return it;
+}
+
+PMO_API int pmo_pagerank_adjoint(int64_t n, const int32_t *off, const int32_t *idx, const double *w,
+                                 double damping, double tol, int max_iters, const double *p,
+                                 const double *g, double *lambda, double *dw) {
+  double *q = (double *)malloc((size_t)n * sizeof(double));
+  memcpy(lambda, g, (size_t)n * sizeof(double));
+  int it = 0;
+  while (it < max_iters) {
+    double r = 0.0, tot = 0.0;
+    for (int64_t s = 0; s < n; ++s) {
+      double acc = 0.0;
+      for (int64_t e = off[s]; e < off[s + 1]; ++e) acc += w[e] * lambda[idx[e]];
+      q[s] = damping * acc + g[s];
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      r += fabs(q[i] - lambda[i]);
+      tot += fabs(q[i]);
+    }
+    memcpy(lambda, q, (size_t)n * sizeof(double));
+    ++it;
+    if (r <= tol * tot) break;
+  }
+  for (int64_t s = 0; s < n; ++s)
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) dw[e] = damping * lambda[idx[e]] * p[s];
+  free(q);
+  return it;
+}
+
+/* One weighted SpMV y = A_W^T x and its backward for cotangent gy:          */
+/* dx[s] = sum_{e=s->v} W_e gy[v],  dW_e = gy[v] * x[s].                     */
+PMO_API void pmo_spmv_backward(int64_t n, const int32_t *off, const int32_t *idx, const double *w,
+                               const double *x, const double *gy, double *dx, double *dw) {
+  for (int64_t s = 0; s < n; ++s) {
+    double acc = 0.0;
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) {
+      acc += w[e] * gy[idx[e]];
+      dw[e] = gy[idx[e]] * x[s];
+    }
+    dx[s] = acc;
+  }
+}
+
+/* Lognormal(0, 1) edge weights normalised per source row (sum 1 over the   */
+/* out-edges of every vertex): z = sqrt(-2 ln u1) cos(2 pi u2) (Box-Muller)  */
+/* from u1 = ((h1 >> 11) + 1) 2^-53, u2 = (h2 >> 11) 2^-53, h1/h2 = hash(seed,*/
+/* 2e), hash(seed, 2e+1).                                                    */
+PMO_API void pmo_lognormal_weights(int64_t n, const int32_t *off, uint64_t seed, double *w) {
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int64_t s = 0; s < n; ++s) {
+    double sum = 0.0;
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) {
+      double u1 = (double)((pmo_hash(seed, 2 * (uint64_t)e) >> 11) + 1) * (1.0 / 9007199254740992.0);
+      double u2 = (double)(pmo_hash(seed, 2 * (uint64_t)e + 1) >> 11) * (1.0 / 9007199254740992.0);
+      w[e] = exp(sqrt(-2.0 * log(u1)) * cos(two_pi * u2));
+      sum += w[e];
+    }
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) w[e] /= sum;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
 /* SpMV (numa-SPMV.C): every iteration pushes over ALL vertices             */
 /* (SPMV_F::updateAtomic numa-SPMV.C:72-81, loop 168-193), then resets      */
 /* p_curr = 0 and swaps, so x_{t+1}[d] = sum_{s->d} w(s,d) * x_t[s].         */

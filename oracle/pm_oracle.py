@@ -67,6 +67,12 @@ def lib():
             "pmo_pagerank": (None, [i64, i32p, i32p, C.c_int, C.c_double, f64p, C.c_void_p]),
             "pmo_spmv": (None, [i64, i32p, i32p, f64p, f64p, C.c_int, f64p]),
             "pmo_ppr": (None, [i64, i32p, i32p, i32p, C.c_int, C.c_int, C.c_double, f64p]),
+            "pmo_weighted_pagerank": (C.c_int, [i64, i32p, i32p, f64p, C.c_double, C.c_double,
+                                                C.c_int, f64p]),
+            "pmo_pagerank_adjoint": (C.c_int, [i64, i32p, i32p, f64p, C.c_double, C.c_double, C.c_int,
+                                               f64p, f64p, f64p, f64p]),
+            "pmo_spmv_backward": (None, [i64, i32p, i32p, f64p, f64p, f64p, f64p, f64p]),
+            "pmo_lognormal_weights": (None, [i64, i32p, u64, f64p]),
             "pmo_er_part_sizes": (i64, [C.c_int, i64, i64, u64, np.ctypeslib.ndpointer(np.int64)]),
             "pmo_er_batch": (i64, [C.c_int, i64, i64, C.c_int, u64, np.ctypeslib.ndpointer(np.int64),
                                    i32p, i32p]),
@@ -200,6 +206,53 @@ def ppr(g: Graph, seeds, iters: int, damping: float = 0.85) -> np.ndarray:
     out = np.empty(g.n * len(s), np.float64)
     lib().pmo_ppr(g.n, g.off, _idx(g), s, len(s), iters, damping, out)
     return out.reshape(g.n, len(s))
+
+
+def lognormal_weights(g: Graph, seed: int = SEED_WEIGHT) -> np.ndarray:
+    """Lognormal(0,1) weights normalised per source row, FP64, CSR order."""
+    w = np.empty(max(g.m, 1), np.float64)
+    lib().pmo_lognormal_weights(g.n, g.off, seed, w)
+    return w[: g.m]
+
+
+def weighted_pagerank(g: Graph, w, damping: float = 0.85, tol: float = 1e-6, max_iters: int = 1000):
+    p = np.empty(g.n, np.float64)
+    it = lib().pmo_weighted_pagerank(g.n, g.off, _idx(g), np.ascontiguousarray(w, np.float64),
+                                     damping, tol, max_iters, p)
+    return p, it
+
+
+def pagerank_adjoint(g: Graph, w, p, gp, damping: float = 0.85, tol: float = 1e-6,
+                     max_iters: int = 1000):
+    """(dL/dW per CSR edge, lambda, iterations) for cotangent gp = dL/dp."""
+    lam = np.empty(g.n, np.float64)
+    dw = np.empty(max(g.m, 1), np.float64)
+    it = lib().pmo_pagerank_adjoint(g.n, g.off, _idx(g), np.ascontiguousarray(w, np.float64), damping,
+                                    tol, max_iters, np.ascontiguousarray(p, np.float64),
+                                    np.ascontiguousarray(gp, np.float64), lam, dw)
+    return dw[: g.m], lam, it
+
+
+def spmv_backward(g: Graph, w, x, gy):
+    dx = np.empty(g.n, np.float64)
+    dw = np.empty(max(g.m, 1), np.float64)
+    lib().pmo_spmv_backward(g.n, g.off, _idx(g), np.ascontiguousarray(w, np.float64),
+                            np.ascontiguousarray(x, np.float64), np.ascontiguousarray(gy, np.float64),
+                            dx, dw)
+    return dx, dw[: g.m]
+
+
+def induced_subgraph(g: Graph, k: int, w=None):
+    """Subgraph on vertices [0, k) keeping the edges between them (and their
+    weights when given)."""
+    src = np.repeat(np.arange(g.n), np.diff(g.off))
+    keep = (src < k) & (g.idx < k)
+    s, d = src[keep], g.idx[keep]
+    off = np.zeros(k + 1, np.int32)
+    np.add.at(off, s + 1, 1)
+    off = np.cumsum(off).astype(np.int32)
+    sub = Graph(k, off, d.astype(np.int32))
+    return (sub, np.asarray(w)[keep]) if w is not None else sub
 
 
 def spmv(g: Graph, w, x0, iters: int) -> np.ndarray:

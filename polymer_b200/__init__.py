@@ -87,6 +87,12 @@ def lib():
         "pm_graph_set_parts": [vp, vp, C.c_int],
         "pm_graph_get_parts": [vp, vp, C.POINTER(C.c_int)],
         "pm_pagerank_parts": [vp, C.c_int, C.c_double, vp, u32],
+        "pm_weighted_pagerank": [vp, C.c_double, C.c_double, C.c_int, vp, u32, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_double)],
+        "pm_pagerank_adjoint": [vp, C.c_double, C.c_double, C.c_int, vp, vp, vp, vp, u32,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double)],
+        "pm_spmv_backward": [vp, vp, vp, vp, vp, u32],
+        "pm_graph_gen_weights_lognormal": [vp, u64],
         "pm_components": [vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
@@ -235,6 +241,10 @@ class Graph:
     def gen_weights_unit(self, seed: int = 0x5EED0002) -> None:
         _check(lib().pm_graph_gen_weights_f32(self._h, seed))
 
+    def gen_weights_lognormal(self, seed: int = 0x5EED0007) -> None:
+        """Lognormal(0,1) float weights normalised per source row."""
+        _check(lib().pm_graph_gen_weights_lognormal(self._h, seed))
+
     def weights_f32(self) -> np.ndarray:
         w = np.empty(max(self.m, 1), np.float32)
         _check(lib().pm_graph_get_weights_f32(self._h, w.ctypes.data_as(C.c_void_p), PM_MEM_HOST))
@@ -366,6 +376,47 @@ def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float6
                              PM_F64 if dt == np.float64 else PM_F32, pr, mem,
                              res.ctypes.data_as(C.c_void_p) if resid else None))
     return (ranks, res[:maxIter]) if resid else ranks
+
+
+def WeightedPageRank(g: Graph, damping: float = 0.85, tol: float = 1e-6, max_iters: int = 1000,
+                     device_out=None, out=None):
+    """p = damping * A_W^T p + (1-damping)/n over the float weights, to a
+    relative L1 change <= tol: (p, iterations, last relative change)."""
+    p, pp, mem = _out(device_out, g.n, np.float32, out)
+    it, res = C.c_int(), C.c_double()
+    _check(lib().pm_weighted_pagerank(g.handle, float(damping), float(tol), int(max_iters), pp, mem,
+                                      C.byref(it), C.byref(res)))
+    return p, it.value, res.value
+
+
+def PageRankAdjoint(g: Graph, p, grad_p, damping: float = 0.85, tol: float = 1e-6,
+                    max_iters: int = 1000, with_lambda: bool = False, out=None):
+    """dL/dW per CSR edge for the cotangent grad_p at the fixed point p
+    (transposed iteration over the CSR): dw (, lambda), iterations."""
+    pp, mem, kp = _arg(p, np.float32)
+    pg, mem2, kg = _arg(grad_p, np.float32)
+    if mem != mem2:
+        raise PolymerError(1, "p and grad_p must live in the same memory space")
+    like = p if mem == PM_MEM_DEVICE else None
+    dw, pdw, _ = _out(like, g.m, np.float32, out)
+    lam, pl, _ = _out(like, g.n, np.float32) if with_lambda else (None, None, None)
+    it, res = C.c_int(), C.c_double()
+    _check(lib().pm_pagerank_adjoint(g.handle, float(damping), float(tol), int(max_iters), pp, pg, pdw,
+                                     pl, mem, C.byref(it), C.byref(res)))
+    return (dw, lam, it.value) if with_lambda else (dw, it.value)
+
+
+def SpMVBackward(g: Graph, x, grad_y):
+    """Backward of y = A_W^T x: (dx = A_W grad_y, dw[e] = grad_y[v] x[s])."""
+    px, mem, kx = _arg(x, np.float32)
+    pg, mem2, kg = _arg(grad_y, np.float32)
+    if mem != mem2:
+        raise PolymerError(1, "x and grad_y must live in the same memory space")
+    like = x if mem == PM_MEM_DEVICE else None
+    dx, pdx, _ = _out(like, g.n, np.float32)
+    dw, pdw, _ = _out(like, g.m, np.float32)
+    _check(lib().pm_spmv_backward(g.handle, px, pg, pdx, pdw, mem))
+    return dx, dw
 
 
 def PageRankParts(g: Graph, maxIter: int = 20, damping: float = 0.85, device_out=None, out=None):

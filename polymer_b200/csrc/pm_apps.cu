@@ -85,7 +85,7 @@ struct CC_F {
     return test_bit(cur, s) ? *((volatile int32_t *)ids + s) : 0x7fffffff;
   }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return min(a, b); }
-  __device__ __forceinline__ bool commit(int d, Acc acc, double &) const {
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
     if (acc < ids[d]) {
       ids[d] = acc;
       return true;
@@ -140,7 +140,7 @@ struct BF_F {
     return test_bit(cur, s) ? *((volatile int32_t *)dist + s) + w : 0x7fffffff;
   }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return min(a, b); }
-  __device__ __forceinline__ bool commit(int d, Acc acc, double &) const {
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
     if (acc < dist[d]) {
       dist[d] = acc;
       return true;
@@ -202,7 +202,7 @@ struct PR_F {
   __device__ __forceinline__ Acc identity() const { return T(-0.0); }
   __device__ __forceinline__ Acc edge(int s, int, int) const { return __ldg(c_cur + s); }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
-  __device__ __forceinline__ bool commit(int d, Acc acc, double &resid) const {
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &resid) const {
     const bool in_f = !signbit(__ldg(c_cur + d));
     const bool hit = !signbit(acc);
     const T old = pc[d];
@@ -214,7 +214,8 @@ struct PR_F {
     pn[d] = nb;
     const int deg = __ldg(out_off + d + 1) - __ldg(out_off + d);
     c_next[d] = hit ? (deg > 0 ? nb / T(deg) : T(0)) : T(-0.0);
-    resid += fabs((double)nb - (double)old);
+    resid.x += fabs((double)nb - (double)old);
+    resid.y += fabs((double)nb);
     return hit;
   }
 };
@@ -269,10 +270,10 @@ struct SPMV_F {
   __device__ __forceinline__ Acc identity() const { return -0.0f; }
   __device__ __forceinline__ Acc edge(int s, int, float w) const { return w * __ldg(x + s); }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
-  __device__ __forceinline__ bool commit(int d, Acc acc, double &norm) const {
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &norm) const {
     const float v = acc + 0.0f;
     y[d] = v;
-    norm += fabs((double)v);
+    norm.x += fabs((double)v);
     return false;
   }
 };
@@ -314,7 +315,7 @@ struct BP_F {
   __device__ __forceinline__ Acc identity() const { return 0; }
   __device__ __forceinline__ Acc edge(int s, int, int) const { return test_bit(cur, s) ? 1 : 0; }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
-  __device__ __forceinline__ bool commit(int d, Acc k, double &) const {
+  __device__ __forceinline__ bool commit(int d, Acc k, double2 &) const {
     const bool in_f = test_bit(cur, d);
     float2 out = in_f ? make_float2(0.f, 0.f) : ln[d];
     if (k > 0) {

@@ -47,7 +47,7 @@ struct MSBFS_F {
   __device__ __forceinline__ Acc identity() const { return 0ull; }
   __device__ __forceinline__ Acc edge(int s, int, int) const { return __ldg(front + s); }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a | b; }
-  __device__ __forceinline__ bool commit(int d, Acc acc, double &) const {
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
     const u64 nb = acc & ~visited[d];
     next[d] = nb;
     if (nb) {

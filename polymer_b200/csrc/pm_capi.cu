@@ -29,6 +29,12 @@ void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out);
 void generate_er_batch(pm_graph *g, int count, int64_t n_min, int64_t n_max, int avg_degree,
                        uint64_t seed);
 void check_parts(pm_graph *g, const std::vector<int64_t> &vbase);
+int run_weighted_pagerank(pm_graph *g, double damping, double tol, int max_iters, float *d_p,
+                          double *resid);
+int run_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters, const float *d_p,
+                         const float *d_g, float *d_dw, float *d_lambda, double *resid);
+void run_spmv_backward(pm_graph *g, const float *d_x, const float *d_gy, float *d_dx, float *d_dw);
+void gen_weights_lognormal(pm_graph *g, uint64_t seed);
 void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
 }  // namespace pm
 
@@ -449,6 +455,89 @@ pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t me
     if (mem == PM_MEM_HOST) from_device(g, y, dy, bytes, mem);
     if (norm1 && iters > 0) from_device(g, norm1, dn, (size_t)iters * 8, PM_MEM_HOST);
     finish(g);
+  });
+}
+
+static void need_weights_f32(pm_graph *g) {
+  need(g->w_f32_out.p != nullptr, "graph has no float weights (pm_graph_set_weights_f32)");
+}
+
+// Device copy of a float input (or the pointer itself for device memory).
+static const float *stage_in(pm_graph *g, const float *x, size_t count, int slot, uint32_t mem) {
+  if (mem == PM_MEM_DEVICE) return x;
+  float *t = (float *)g->scratch_buf(slot, count * 4);
+  to_device(g, t, x, count * 4, mem);
+  return t;
+}
+
+pm_status pm_weighted_pagerank(pm_graph *g, double damping, double tol, int max_iters, float *p,
+                               uint32_t mem, int *iters, double *resid) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(p != nullptr, "null p");
+    need(max_iters >= 1 && tol >= 0, "need max_iters >= 1 and tol >= 0");
+    need_weights_f32(g);
+    const size_t bytes = (size_t)g->n * 4;
+    float *dp = mem == PM_MEM_DEVICE ? p : (float *)g->scratch_buf(kSlotOut0, bytes);
+    const int it = run_weighted_pagerank(g, damping, tol, max_iters, dp, resid);
+    if (iters) *iters = it;
+    if (mem == PM_MEM_HOST) from_device(g, p, dp, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters, const float *p,
+                              const float *grad_p, float *dw, float *lambda, uint32_t mem, int *iters,
+                              double *resid) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(p != nullptr && grad_p != nullptr && dw != nullptr, "null p/grad_p/dw");
+    need(max_iters >= 1 && tol >= 0, "need max_iters >= 1 and tol >= 0");
+    need_weights_f32(g);
+    const size_t n = (size_t)g->n, m = (size_t)g->m;
+    const float *dp = stage_in(g, p, n, kSlotIn0, mem);
+    const float *dg = stage_in(g, grad_p, n, kSlotIn1, mem);
+    float *ddw = mem == PM_MEM_DEVICE ? dw : (float *)g->scratch_buf(kSlotOut0, std::max<size_t>(m, 1) * 4);
+    float *dl = lambda == nullptr ? nullptr
+                : mem == PM_MEM_DEVICE ? lambda : (float *)g->scratch_buf(kSlotOut1, n * 4);
+    const int it = run_pagerank_adjoint(g, damping, tol, max_iters, dp, dg, ddw, dl, resid);
+    if (iters) *iters = it;
+    if (mem == PM_MEM_HOST) {
+      from_device(g, dw, ddw, m * 4, mem);
+      if (lambda) from_device(g, lambda, dl, n * 4, mem);
+    }
+    finish(g);
+  });
+}
+
+pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, float *dx, float *dw,
+                           uint32_t mem) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(x != nullptr && grad_y != nullptr, "null x/grad_y");
+    need_weights_f32(g);
+    const size_t n = (size_t)g->n, m = (size_t)g->m;
+    const float *dx_in = stage_in(g, x, n, kSlotIn0, mem);
+    const float *dgy = stage_in(g, grad_y, n, kSlotIn1, mem);
+    float *ddx = dx == nullptr ? nullptr : mem == PM_MEM_DEVICE ? dx : (float *)g->scratch_buf(kSlotOut0, n * 4);
+    float *ddw = dw == nullptr ? nullptr
+                 : mem == PM_MEM_DEVICE ? dw : (float *)g->scratch_buf(kSlotOut1, std::max<size_t>(m, 1) * 4);
+    run_spmv_backward(g, dx_in, dgy, ddx, ddw);
+    if (mem == PM_MEM_HOST) {
+      if (dx) from_device(g, dx, ddx, n * 4, mem);
+      if (dw) from_device(g, dw, ddw, m * 4, mem);
+    }
+    finish(g);
+  });
+}
+
+pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed) {
+  return guard([&] {
+    enter(g);
+    gen_weights_lognormal(g, seed);
   });
 }
 

@@ -113,6 +113,7 @@ struct Counters {
   unsigned long long edges;
   unsigned long long aux;  // algorithm-specific (e.g. edges inspected)
   double daux;             // FP64 reductions (residuals, norms)
+  double daux2;            // a second one (the norm of a relative residual)
   unsigned int err;
   unsigned int pad;
 };

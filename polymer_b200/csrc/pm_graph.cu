@@ -290,8 +290,10 @@ void finish_graph(pm_graph *g) {
   g->queue1.alloc((size_t)(n + 1) * 4);
   g->defer.alloc((size_t)(n + 1) * 4);
   g->hubs.alloc((size_t)kMaxHubs * 4);
-  g->partials.alloc((size_t)std::max(v.in.nchunks, 1) * 16);
+  // partial sums of heavy chunks, for pulls over the CSC or over the CSR
+  g->partials.alloc((size_t)std::max(std::max(v.in.nchunks, v.out.nchunks), 1) * 16);
   g->cnt.alloc(3 * sizeof(Counters));
+  PM_CUDA(cudaMemsetAsync(g->cnt.p, 0, 3 * sizeof(Counters), st));  // error words start clear
   g->E.d_cnt = g->cnt.as<Counters>();
   g->E.defer = g->defer.as<int32_t>();
   g->E.hubs = g->hubs.as<int32_t>();
@@ -526,6 +528,38 @@ void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float) {
                      seed, wmax, g->w_i32_out.as<int32_t>());
     permute_weights_i32(g);
   }
+}
+
+void ensure_out_src(pm_graph *g) {
+  if (g->out_src.p) return;
+  g->out_src.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
+  if (g->m)
+    PM_LAUNCH(k_edge_src, grid1d(g->m), 256, 0, g->E.stream, g->out.off.as<int32_t>(), g->n, g->m,
+              g->out_src.as<int32_t>());
+}
+
+// Lognormal(0,1) weights normalised per source row (the oracle's
+// pmo_lognormal_weights rule, evaluated in FP32 with CUDA's libm).
+__global__ void k_lognormal_rows(const int32_t *off, int64_t n, uint64_t seed, float *w) {
+  const float two_pi = 6.28318530717958647692f;
+  GRID_STRIDE(s, n) {
+    float sum = 0.0f;
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) {
+      const double u1 = (double)((hash64(seed, 2 * (uint64_t)e) >> 11) + 1) * (1.0 / 9007199254740992.0);
+      const double u2 = (double)(hash64(seed, 2 * (uint64_t)e + 1) >> 11) * (1.0 / 9007199254740992.0);
+      const float x = expf(sqrtf(-2.0f * logf((float)u1)) * cosf(two_pi * (float)u2));
+      w[e] = x;
+      sum += x;
+    }
+    for (int64_t e = off[s]; e < off[s + 1]; ++e) w[e] /= sum;
+  }
+}
+
+void gen_weights_lognormal(pm_graph *g, uint64_t seed) {
+  g->w_f32_out.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
+  PM_LAUNCH(k_lognormal_rows, grid1d(g->n), 256, 0, g->E.stream, g->out.off.as<int32_t>(), g->n, seed,
+            g->w_f32_out.as<float>());
+  permute_weights_f32(g);
 }
 
 void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count) {

@@ -70,6 +70,7 @@ struct pm_graph {
   int32_t max_out_deg = 0;
   pm::AdjBuf out, in;     // in.* empty when symmetric (views alias out)
   pm::DevBuf in_eid;      // CSC slot -> CSR edge id (directed graphs)
+  pm::DevBuf out_src;     // source of every CSR edge (built on first use)
   pm::DevBuf w_i32_out, w_i32_in, w_f32_out, w_f32_in;
   pm::Engine E;
   pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials;

@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(kPullBlock) k_pull_reduce(GraphView g, F f, co
   int *pos_s = s_pos[wid];
   int *off_s = s_off[wid];
   unsigned long long my_size = 0, my_edges = 0;
-  double my_aux = 0.0;
+  double2 my_aux = make_double2(0.0, 0.0);
   // persistent warps: each takes the next group from a ticket counter
   for (;;) {
   int grp = 0;
@@ -614,13 +614,15 @@ __global__ void __launch_bounds__(kPullBlock) k_pull_reduce(GraphView g, F f, co
   }  // group loop
   my_size = warp_sum(my_size);
   my_edges = warp_sum(my_edges);
-  my_aux = warp_sum(my_aux);
+  my_aux.x = warp_sum(my_aux.x);
+  my_aux.y = warp_sum(my_aux.y);
   if (lane == 0) {
     if (my_size) {
       atomicAdd(&cnt->size, my_size);
       atomicAdd(&cnt->edges, my_edges);
     }
-    if (my_aux != 0.0) atomicAdd(&cnt->daux, my_aux);
+    if (my_aux.x != 0.0) atomicAdd(&cnt->daux, my_aux.x);
+    if (my_aux.y != 0.0) atomicAdd(&cnt->daux2, my_aux.y);
   }
 }
 
