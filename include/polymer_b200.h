@@ -242,6 +242,26 @@ PM_API pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed);
 PM_API pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
                 uint32_t mem);
 
+/* PageRank for callers that cannot allocate GPU memory.  No counterpart in
+ * the reference.  Some hosts may not call cudaMalloc while they run (a
+ * plugin in a process whose device memory another runtime pools, a caller
+ * that gave all device memory to its own allocator); every other entry point
+ * here allocates (a graph handle owns its CSC, tables and workspaces).  This
+ * one allocates nothing: offsets (n+1) and edges (m) are a CSR already in
+ * device memory, ranks (n floats) is a device output, and the working
+ * vectors live in a fixed array inside the library, sized for at most
+ * 1048576 vertices (about 8.3 MB, held on every GPU that loads the library
+ * until the process exits); larger n is rejected with PM_ERR_INVALID_ARG.
+ * Semantics are pm_pagerank's with PM_F32 (the graph must have no self
+ * loops); pushes use atomics, so sums may differ from pm_pagerank in the
+ * last bits.  Runs on `stream` (NULL = default stream) of the current device
+ * and returns when done.  The first call on a device looks up the array's
+ * address for that device; make it before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU race. */
+PM_API pm_status pm_pagerank_static(const int32_t *offsets, const int32_t *edges, int64_t n,
+                                    int64_t m, int iters, double damping, float *ranks,
+                                    void *stream);
+
 /* Device timing on the graph's stream (CUDA events): begin, then end
  * returns the elapsed milliseconds. */
 PM_API pm_status pm_timer_begin(pm_graph *g);

@@ -93,6 +93,7 @@ def lib():
                                 C.POINTER(C.c_int), C.POINTER(C.c_double)],
         "pm_spmv_backward": [vp, vp, vp, vp, vp, u32],
         "pm_graph_gen_weights_lognormal": [vp, u64],
+        "pm_pagerank_static": [vp, vp, i64, i64, C.c_int, C.c_double, vp, vp],
         "pm_components": [vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
@@ -417,6 +418,22 @@ def SpMVBackward(g: Graph, x, grad_y):
     dw, pdw, _ = _out(like, g.m, np.float32)
     _check(lib().pm_spmv_backward(g.handle, px, pg, pdx, pdw, mem))
     return dx, dw
+
+
+def PageRankStatic(offsets, edges, ranks, maxIter: int = 20, damping: float = 0.85, stream=None):
+    """PageRank for callers that cannot allocate GPU memory (pm_pagerank_static):
+    offsets (n+1), edges (m) and ranks (n, float32) are CUDA tensors; the
+    working vectors live in a fixed array inside the library (n <= 2^20).
+    Nothing is allocated by this call."""
+    for t in (offsets, edges, ranks):
+        if not _is_device(t):
+            raise PolymerError(1, "PageRankStatic takes CUDA tensors only")
+    n = offsets.numel() - 1
+    _check(lib().pm_pagerank_static(C.c_void_p(offsets.data_ptr()), C.c_void_p(edges.data_ptr()), n,
+                                    edges.numel(), int(maxIter), float(damping),
+                                    C.c_void_p(ranks.data_ptr()),
+                                    None if stream is None else C.c_void_p(stream)))
+    return ranks
 
 
 def PageRankParts(g: Graph, maxIter: int = 20, damping: float = 0.85, device_out=None, out=None):

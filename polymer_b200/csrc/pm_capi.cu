@@ -42,6 +42,10 @@ using namespace pm;
 
 static thread_local std::string t_last_error;
 
+namespace pm {
+void set_last_error(const std::string &msg) { t_last_error = msg; }
+}  // namespace pm
+
 // Scratch slots used for staging at the boundary (the algorithms use 0..3).
 enum { kSlotIn0 = 8, kSlotIn1 = 9, kSlotOut0 = 10, kSlotOut1 = 11, kSlotAux = 12 };
 

@@ -18,6 +18,7 @@ struct Failure : std::runtime_error {
 };
 
 [[noreturn]] void fail(pm_status s, const std::string &msg);
+void set_last_error(const std::string &msg);  // text returned by pm_last_error()
 [[noreturn]] void fail_cuda(cudaError_t e, const char *what, const char *file, int line);
 void count_launch(int n = 1);
 
