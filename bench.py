@@ -265,8 +265,11 @@ def e2e_run(pm, suite, steps):
 
 
 def batched_block(pm, suite, reps=3):
-    """configs[3] workloads against plain runs on the same GPU: 64-source BFS
-    (uint64 lanes) vs 64 single-source BFS; device time by CUDA events."""
+    """Batched workloads against plain runs on the same GPU, device time by
+    CUDA events: 64-source BFS (uint64 lanes) vs 64 single-source BFS, 64-source
+    BellmanFord (int32 lanes) vs 64 single-source runs, personalised PageRank
+    for 32 seeds vs 32 plain runs, PageRank on 256 ER graphs in one launch vs
+    256 launches."""
     A = suite.A
     offA, _ = A.csr()
     src64 = suite._pick_sources(offA, 64, SEED_SRC + 100)
@@ -286,6 +289,25 @@ def batched_block(pm, suite, reps=3):
     res = {"bfs64": {"ms": round(t, 3), "gteps": round(st["edges_visited"] / (t / 1e3) / 1e9, 2),
                      "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
                      "graph": "symmetrised R-MAT scale %d" % int(np.log2(A.n))}}
+    # 64-source BellmanFord over the same graph's int32 weights (1..22)
+    pm.BellmanFordMulti(src64, A, device_out=out, out=out)
+    ms_multi = []
+    for _ in range(reps):
+        A.timer_begin()
+        _, st = pm.BellmanFordMulti(src64, A, device_out=out, out=out, stats=True)
+        ms_multi.append(A.timer_end())
+    ms_plain, edges_plain = 0.0, 0
+    for s in src64:
+        A.timer_begin()
+        _, st1 = pm.BellmanFord(A, s, device_out=suite.outA, stats=True)
+        ms_plain += A.timer_end()
+        edges_plain += st1["edges_visited"]
+    t = statistics.median(ms_multi)
+    res["bf64"] = {"ms": round(t, 3), "rounds": st["rounds"], "dense_rounds": st["dense_rounds"],
+                   "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
+                   "plain_gteps": round(edges_plain / (ms_plain / 1e3) / 1e9, 2),
+                   "gteps_equiv": round(edges_plain / (t / 1e3) / 1e9, 2),
+                   "note": "gteps_equiv = edges the 64 plain runs visit / multi-source time"}
     # personalised PageRank, 32 one-hot seeds, 20 iterations, n x 32 FP32
     B = suite.B
     offB, _ = B.csr()
@@ -331,7 +353,7 @@ def batched_block(pm, suite, reps=3):
 
 
 def adjoint_block(pm, torch, dev, reps=3):
-    """weighted PageRank on directed R-MAT scale 20 with
+    """Weighted PageRank on directed R-MAT scale 20 with
     lognormal(0,1) weights normalised per source row, damping 0.85, solved to
     1e-6 relative L1; loss = sum of the ranks of 1024 seeded targets; adjoint
     (transposed iteration + per-edge gradient) vs forward solve, and the
@@ -583,7 +605,7 @@ def main():
     pass_ms = pr_ms / max(pr_passes, 1)
     achieved = pass_bytes / (pass_ms / 1e3) / 1e9 if pr_passes else None
     per_algo = {}
-    algo_bytes = {  # algorithmic bytes per counted edge-unit, see DESIGN.md
+    algo_bytes = {  # algorithmic bytes of each application's passes
         "pagerank": lambda: (8 * mB + 32 * nB) * 20, "spmv": lambda: (12 * mB + 12 * nB) * 10,
         "bp": lambda: (4 * mB + 40 * nB) * 10,
     }

@@ -164,6 +164,19 @@ PM_API pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64
 PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem,
                           int64_t threshold, pm_traversal_stats *stats);
 
+/* Multi-source BellmanFord: k <= 64 sources in one traversal, 64 int32
+ * distance lanes per vertex (BF_F of numa-BellmanFord.C:61-85 per lane; the
+ * reference runs one source per process).  The frontier is the set of
+ * vertices with a lane that fell in the last round; the direction rule of
+ * pm_bellman_ford applies to it (threshold < 0 selects m/20).  dist: k*n
+ * int32, source-major (dist[l*n + v] = distance of v from sources[l],
+ * 1073741823 when unreached) -- each row equals pm_bellman_ford's dist for
+ * that source.  sources: k int32 in mem's space.  stats->reached = number of
+ * (source, vertex) pairs reached; stats->edges_visited = sum over rounds of
+ * the frontier's out-degrees. */
+PM_API pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dist,
+                                       uint32_t mem, int64_t threshold, pm_traversal_stats *stats);
+
 /* PageRank with Polymer's frontier semantics.  Replaces PageRank(GA,
  * maxIter) (numa-PageRank.C:548) with PR_F / PR_Vertex_F / PR_Vertex_Reset
  * (64-148) and the loop at 273-335: p = 1/n on all vertices, each iteration

@@ -24,7 +24,8 @@ import os
 import numpy as np
 
 __all__ = [
-    "Graph", "PolymerError", "PageRank", "BFS", "BFSMulti", "Components", "BellmanFord", "SPMV",
+    "Graph", "PolymerError", "PageRank", "BFS", "BFSMulti", "Components", "BellmanFord",
+    "BellmanFordMulti", "SPMV",
     "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
 ]
 
@@ -82,6 +83,7 @@ def lib():
         "pm_fill_uniform_f32": [vp, u64, C.c_int, vp, i64],
         "pm_bfs": [vp, i32, vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bfs_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_bellman_ford_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_ppr": [vp, vp, C.c_int, C.c_int, C.c_double, vp, u32],
         "pm_graph_create_er_batch": [C.c_int, i64, i64, C.c_int, u64, C.c_int, C.POINTER(vp)],
         "pm_graph_set_parts": [vp, vp, C.c_int],
@@ -330,24 +332,36 @@ def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool 
     return (par, dep, st.as_dict()) if stats else (par, dep)
 
 
-def BFSMulti(sources, g: Graph, threshold: int = -1, device_out=None, stats: bool = False,
-             out=None):
-    """Depths from up to 64 sources in one traversal (uint64 source lanes per
-    vertex): a (k, n) int32 array, row l = BFS depths from sources[l]."""
+def _multi_source(fn, sources, g: Graph, threshold, device_out, stats, out):
     src = np.ascontiguousarray(sources, np.int32)
     k = len(src)
-    dep, pd, mem = _out(device_out, k * g.n, np.int32, None if out is None else out.reshape(-1))
+    res, pd, mem = _out(device_out, k * g.n, np.int32, None if out is None else out.reshape(-1))
     if mem == PM_MEM_DEVICE:
         import torch
-        src_t = torch.from_numpy(src).to(dep.device)
+        src_t = torch.from_numpy(src).to(res.device)
         ps = C.c_void_p(src_t.data_ptr())
         torch.cuda.synchronize()
     else:
         ps = src.ctypes.data_as(C.c_void_p)
     st = TraversalStats()
-    _check(lib().pm_bfs_multi(g.handle, ps, k, pd, mem, int(threshold), C.byref(st)))
-    dep = dep.reshape(k, g.n)
-    return (dep, st.as_dict()) if stats else dep
+    _check(fn(g.handle, ps, k, pd, mem, int(threshold), C.byref(st)))
+    res = res.reshape(k, g.n)
+    return (res, st.as_dict()) if stats else res
+
+
+def BFSMulti(sources, g: Graph, threshold: int = -1, device_out=None, stats: bool = False,
+             out=None):
+    """Depths from up to 64 sources in one traversal (uint64 source lanes per
+    vertex): a (k, n) int32 array, row l = BFS depths from sources[l]."""
+    return _multi_source(lib().pm_bfs_multi, sources, g, threshold, device_out, stats, out)
+
+
+def BellmanFordMulti(sources, g: Graph, threshold: int = -1, device_out=None, stats: bool = False,
+                     out=None):
+    """Shortest-path distances from up to 64 sources in one traversal (64
+    int32 distance lanes per vertex): a (k, n) int32 array, row l = the
+    BellmanFord distances from sources[l]."""
+    return _multi_source(lib().pm_bellman_ford_multi, sources, g, threshold, device_out, stats, out)
 
 
 def Components(g: Graph, threshold: int = -1, device_out=None, stats: bool = False, out=None):

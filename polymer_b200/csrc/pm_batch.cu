@@ -1,6 +1,10 @@
-// pm_batch.cu -- batched workloads on the engine: multi-source BFS with one
-// bit per source in a uint64 word per vertex.
+// pm_batch.cu -- batched workloads: multi-source BFS (one bit per source in a
+// uint64 word per vertex), multi-source BellmanFord (64 int32 distance lanes
+// per vertex), personalised PageRank for 32 seeds, and PageRank on every part
+// of a disjoint union in one persistent launch.
 #include <cooperative_groups.h>
+
+#include <cub/cub.cuh>
 
 #include "pm_graph.cuh"
 
@@ -138,6 +142,323 @@ void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, i
   const Counters *h = E.read_counters();
   s.reached = (int64_t)h[2].size;
   s.edges_visited = (int64_t)h[2].edges;
+  if (st) *st = s;
+}
+
+// ===========================================================================
+// Multi-source BellmanFord, up to 64 sources (BF_F of numa-BellmanFord.C:
+// 61-85 with one int32 distance lane per source).  dist is vertex-major,
+// 64 lanes per vertex (256 bytes, one warp-wide pair of 128-byte rows);
+// active[v] has bit l set when lane l of v fell in the last round.  A round
+// follows BF's direction rule on the union frontier (|F| + outdeg(F) >=
+// threshold is dense):
+//  * dense: a warp owns a CSC row, thread t owns lanes t and t+32; for each
+//    in-edge whose source has active lanes it gathers the source's row and
+//    relaxes those lanes; the row's new active word is written in full;
+//  * sparse: the frontier's out-edges are cut into 32-edge chunks (a scan of
+//    the queued out-degrees); for each edge the warp relaxes the active lanes
+//    of the target with atomicMin and ORs the lanes that fell into the
+//    target's next active word.
+// Distances only fall, so reading a row another warp is lowering in the same
+// round is harmless: the lower value is a real path length and the lane that
+// fell is in the next frontier either way.
+// ===========================================================================
+constexpr int kLanes = 64;
+
+// active -> queue of frontier vertices with out-edges (and their degrees);
+// c->size = |F|, c->edges = outdeg(F), c->aux = queue length.
+__global__ void k_bf_multi_frontier(const u64 *__restrict__ active, const int32_t *__restrict__ out_off,
+                                    int64_t n, int32_t *__restrict__ queue, int32_t *__restrict__ qdeg,
+                                    Counters *c) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  unsigned long long size = 0, edges = 0;
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n;
+       base += warps * 32) {
+    const int64_t v = base + lane;
+    int deg = 0;
+    bool act = false;
+    if (v < n) {
+      act = active[v] != 0ull;
+      if (act) deg = __ldg(out_off + v + 1) - __ldg(out_off + v);
+    }
+    size += act;
+    edges += (unsigned)deg;
+    const unsigned push = __ballot_sync(0xffffffffu, deg > 0);
+    if (push) {
+      unsigned long long pos = 0;
+      if (lane == 0) pos = atomicAdd(&c->aux, (unsigned long long)__popc(push));
+      pos = shfl_idx(pos, 0) + __popc(push & ((1u << lane) - 1u));
+      if (deg > 0) {
+        queue[pos] = (int32_t)v;
+        qdeg[pos] = deg;
+      }
+    }
+  }
+  size = warp_sum(size);
+  edges = warp_sum(edges);
+  if (lane == 0 && size) {
+    atomicAdd(&c->size, size);
+    atomicAdd(&c->edges, edges);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_bf_multi_push(const int32_t *__restrict__ out_off,
+                                                       const int32_t *__restrict__ out_idx,
+                                                       const int32_t *__restrict__ w_out,
+                                                       const int32_t *__restrict__ queue,
+                                                       const int32_t *__restrict__ qoff, int q, int64_t total,
+                                                       int32_t *dist, const u64 *__restrict__ active,
+                                                       u64 *next_active) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t chunk = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); chunk * 32 < total;
+       chunk += warps) {
+    const int64_t t0 = chunk * 32;
+    // last queue entry whose first edge is <= t0 (qoff is increasing: every
+    // queued vertex has at least one out-edge)
+    int lo = 0, hi = q - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(qoff + mid) <= t0) lo = mid;
+      else hi = mid - 1;
+    }
+    // queue entries starting inside the chunk mark their first position
+    const int bi = lo + 1 + lane;
+    unsigned start = 0;
+    if (bi < q) {
+      const int64_t p = (int64_t)__ldg(qoff + bi) - t0;
+      if (p < 32) start = 1u << p;
+    }
+    start = __reduce_or_sync(0xffffffffu, start);
+    const int64_t t = t0 + lane;
+    const bool valid = t < total;
+    int s = -1, d = 0;
+    int32_t w = 0;
+    if (valid) {
+      const int qi = lo + __popc(start << (31 - lane));
+      s = __ldg(queue + qi);
+      const int64_t e = (int64_t)__ldg(out_off + s) + (t - __ldg(qoff + qi));
+      d = __ldg(out_idx + e);
+      w = __ldg(w_out + e);
+    }
+    const int cnt = (int)min((int64_t)32, total - t0);
+    int cur = -1;
+    u64 a = 0;
+    int32_t slo = 0, shi = 0;
+    for (int j = 0; j < cnt; ++j) {
+      const int sj = __shfl_sync(0xffffffffu, s, j);
+      const int dj = __shfl_sync(0xffffffffu, d, j);
+      const int32_t wj = __shfl_sync(0xffffffffu, w, j);
+      if (sj != cur) {
+        cur = sj;
+        a = __ldg(active + sj);
+        slo = dist[(int64_t)sj * kLanes + lane];
+        shi = dist[(int64_t)sj * kLanes + 32 + lane];
+      }
+      bool fell_lo = false, fell_hi = false;
+      if ((a >> lane) & 1ull) {
+        int32_t *p = dist + (int64_t)dj * kLanes + lane;
+        const int32_t nv = slo + wj;
+        if (nv < *(volatile int32_t *)p) fell_lo = nv < atomicMin(p, nv);
+      }
+      if ((a >> (32 + lane)) & 1ull) {
+        int32_t *p = dist + (int64_t)dj * kLanes + 32 + lane;
+        const int32_t nv = shi + wj;
+        if (nv < *(volatile int32_t *)p) fell_hi = nv < atomicMin(p, nv);
+      }
+      const u64 mask = (u64)__ballot_sync(0xffffffffu, fell_lo) | ((u64)__ballot_sync(0xffffffffu, fell_hi) << 32);
+      if (lane == 0 && mask) atomicOr(next_active + dj, mask);
+    }
+  }
+}
+
+// Relaxes lanes lo / hi of row v over in-edges [e0, e1) whose sources have
+// active lanes (one warp; thread t owns lanes t and t + 32).
+__device__ __forceinline__ void bf_multi_relax(const int32_t *__restrict__ in_idx,
+                                               const int32_t *__restrict__ w_in, const int32_t *dist,
+                                               const u64 *__restrict__ active, int64_t e0, int64_t e1,
+                                               int32_t &lo, int32_t &hi) {
+  const int lane = lane_id();
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    int s = 0;
+    u64 act = 0;
+    if (e < e1) {
+      s = __ldg(in_idx + e);
+      act = __ldg(active + s);
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, act != 0);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int sj = __shfl_sync(0xffffffffu, s, j);
+      const u64 aj = shfl_idx(act, j);
+      const int32_t wj = __ldg(w_in + base + j);
+      if ((aj >> lane) & 1ull) lo = min(lo, dist[(int64_t)sj * kLanes + lane] + wj);
+      if ((aj >> (32 + lane)) & 1ull) hi = min(hi, dist[(int64_t)sj * kLanes + 32 + lane] + wj);
+    }
+  }
+}
+
+constexpr int kBfPiece = 512;  // in-edges of one warp's piece of a heavy row
+
+// Dense round.  Persistent warps take tickets: the first ones are 512-edge
+// pieces of the heavy rows (in-degree > kHeavyDeg; they lower the row with
+// atomicMin and OR the fallen lanes into next_active, which starts at zero),
+// the rest are merge-path row groups whose light rows each warp relaxes in
+// full and whose next_active words it writes.
+__global__ void __launch_bounds__(256) k_bf_multi_pull(GraphView g, const int32_t *__restrict__ w_in,
+                                                       int32_t *dist, const u64 *__restrict__ active,
+                                                       u64 *next_active, int64_t heavy_pieces,
+                                                       Counters *cnt) {
+  const int lane = lane_id();
+  for (;;) {
+    long long t = 0;
+    if (lane == 0) t = (long long)atomicAdd(&cnt->aux, 1ull);
+    t = shfl_idx(t, 0);
+    if (t < heavy_pieces) {
+      const int c = (int)(t / (kChunkEdges / kBfPiece));
+      const int piece = (int)(t % (kChunkEdges / kBfPiece));
+      const int r = __ldg(g.in.hrow + c);
+      const int64_t row_end = __ldg(g.in.off + r + 1);
+      const int64_t e0 = (int64_t)__ldg(g.in.off + r) +
+                         (int64_t)(c - __ldg(g.in.hfirst + r)) * kChunkEdges + (int64_t)piece * kBfPiece;
+      if (e0 >= row_end) continue;
+      const int64_t e1 = min(e0 + kBfPiece, row_end);
+      int32_t lo = kDevBFInf, hi = kDevBFInf;
+      bf_multi_relax(g.in.idx, w_in, dist, active, e0, e1, lo, hi);
+      bool fell_lo = false, fell_hi = false;
+      int32_t *p = dist + (int64_t)r * kLanes + lane;
+      if (lo < *(volatile int32_t *)p) fell_lo = lo < atomicMin(p, lo);
+      if (hi < *(volatile int32_t *)(p + 32)) fell_hi = hi < atomicMin(p + 32, hi);
+      const u64 mask = (u64)__ballot_sync(0xffffffffu, fell_lo) | ((u64)__ballot_sync(0xffffffffu, fell_hi) << 32);
+      if (lane == 0 && mask) atomicOr(next_active + r, mask);
+      continue;
+    }
+    const long long grp = t - heavy_pieces;
+    if (grp >= g.in.ngroups) break;
+    const int r0 = __ldg(g.in.gstart + grp), r1 = __ldg(g.in.gstart + grp + 1);
+    for (int v = r0; v < r1; ++v) {
+      const int e0 = __ldg(g.in.off + v), e1 = __ldg(g.in.off + v + 1);
+      if (e1 - e0 > kHeavyDeg) continue;
+      const int32_t old_lo = dist[(int64_t)v * kLanes + lane];
+      const int32_t old_hi = dist[(int64_t)v * kLanes + 32 + lane];
+      int32_t lo = old_lo, hi = old_hi;
+      bf_multi_relax(g.in.idx, w_in, dist, active, e0, e1, lo, hi);
+      const unsigned ch_lo = __ballot_sync(0xffffffffu, lo < old_lo);
+      const unsigned ch_hi = __ballot_sync(0xffffffffu, hi < old_hi);
+      if (lo < old_lo) dist[(int64_t)v * kLanes + lane] = lo;
+      if (hi < old_hi) dist[(int64_t)v * kLanes + 32 + lane] = hi;
+      if (lane == 0) next_active[v] = (u64)ch_lo | ((u64)ch_hi << 32);
+    }
+  }
+}
+
+__global__ void k_bf_multi_init(int32_t *dist, u64 *active, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * kLanes; i += stride)
+    dist[i] = kDevBFInf;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) active[i] = 0ull;
+}
+
+__global__ void k_bf_multi_seed(const int32_t *sources, int k, int32_t *dist, u64 *active) {
+  const int l = threadIdx.x;
+  if (l < k) {
+    const int v = sources[l];
+    dist[(int64_t)v * kLanes + l] = 0;
+    atomicOr(active + v, 1ull << l);
+  }
+}
+
+// dist vertex-major (n x 64) -> out source-major (k x n), through 32x32
+// tiles; c->size counts the finite distances (reached (source, vertex) pairs).
+__global__ void k_bf_multi_transpose(const int32_t *__restrict__ dist, int64_t n, int k,
+                                     int32_t *__restrict__ out, Counters *c) {
+  __shared__ int32_t tile[32][33];
+  const int64_t v0 = (int64_t)blockIdx.x * 32;
+  const int l0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t v = v0 + r;
+    tile[r][threadIdx.x] = v < n ? dist[v * kLanes + l0 + threadIdx.x] : kDevBFInf;
+  }
+  __syncthreads();
+  unsigned long long reached = 0;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int l = l0 + r;
+    const int64_t v = v0 + threadIdx.x;
+    if (l < k && v < n) {
+      const int32_t x = tile[threadIdx.x][r];
+      out[(int64_t)l * n + v] = x;
+      reached += x < kDevBFInf;
+    }
+  }
+  reached = warp_sum(reached);
+  if (lane_id() == 0 && reached) atomicAdd(&c->size, reached);
+}
+
+void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_out, int64_t threshold,
+                  pm_traversal_stats *st) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  int32_t *dist = (int32_t *)g->scratch_buf(0, (size_t)n * kLanes * 4);
+  u64 *act = (u64 *)g->scratch_buf(1, (size_t)n * 8);
+  u64 *nxt = (u64 *)g->scratch_buf(2, (size_t)n * 8);
+  int32_t *qdeg = (int32_t *)g->scratch_buf(3, (size_t)n * 4);
+  int32_t *qoff = (int32_t *)g->scratch_buf(4, (size_t)n * 4);
+  int32_t *queue = g->subset(0).queue;
+  size_t tmp_bytes = 0;
+  PM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, qdeg, qoff, (int)n, E.stream));
+  void *tmp = g->scratch_buf(5, std::max<size_t>(tmp_bytes, 16));
+  PM_LAUNCH(k_bf_multi_init, E.grid_for(n * kLanes, 256, 16), 256, 0, E.stream, dist, act, n);
+  PM_LAUNCH(k_bf_multi_seed, 1, 64, 0, E.stream, d_sources, k, dist, act);
+  static int pull_per_sm = 0, push_per_sm = 0;
+  if (pull_per_sm == 0) {
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pull_per_sm, k_bf_multi_pull, 256, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&push_per_sm, k_bf_multi_push, 256, 0));
+    pull_per_sm = std::max(pull_per_sm, 1);
+    push_per_sm = std::max(push_per_sm, 1);
+  }
+  const int64_t heavy_pieces = (int64_t)E.g.in.nchunks * (kChunkEdges / kBfPiece);
+  const int pull_grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>((heavy_pieces + E.g.in.ngroups + 7) / 8, (int64_t)E.num_sms * pull_per_sm));
+  const int32_t *w_in = g->w_i32_in.as<int32_t>(), *w_out = g->w_i32_out.as<int32_t>();
+  pm_traversal_stats s{};
+  E.tag = "bellman_ford_multi";
+  for (;;) {
+    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, 3 * sizeof(Counters), E.stream));
+    PM_LAUNCH(k_bf_multi_frontier, E.grid_for(n, 256, 8), 256, 0, E.stream, act, E.g.out.off, n, queue, qdeg,
+              E.d_cnt + 1);
+    const Counters *h = E.read_counters();
+    const int64_t size = (int64_t)h[1].size, edges = (int64_t)h[1].edges, q = (int64_t)h[1].aux;
+    if (size == 0) break;
+    if (s.rounds > n + 1) fail(PM_ERR_INVALID_ARG, "BellmanFord did not converge");
+    s.edges_visited += edges;
+    const bool dense = size + edges >= threshold;
+    E.prof.begin(E.tag, E.stream);
+    PM_CUDA(cudaMemsetAsync(nxt, 0, (size_t)n * 8, E.stream));
+    if (dense) {
+      PM_LAUNCH(k_bf_multi_pull, pull_grid, 256, 0, E.stream, E.g, w_in, dist, act, nxt, heavy_pieces,
+                E.d_cnt);
+    } else {
+      if (q > 0) {
+        PM_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, qdeg, qoff, (int)q, E.stream));
+        const int64_t chunks = (edges + 31) / 32;
+        const int grid = (int)std::max<int64_t>(
+            1, std::min<int64_t>((chunks + 7) / 8, (int64_t)E.num_sms * push_per_sm));
+        PM_LAUNCH(k_bf_multi_push, grid, 256, 0, E.stream, E.g.out.off, E.g.out.idx, w_out, queue, qoff, (int)q,
+                  edges, dist, act, nxt);
+      }
+    }
+    E.prof.end(E.stream);
+    s.rounds++;
+    s.dense_rounds += dense;
+    std::swap(act, nxt);
+  }
+  PM_CUDA(cudaMemsetAsync(E.d_cnt + 2, 0, sizeof(Counters), E.stream));
+  dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), 2);
+  PM_LAUNCH(k_bf_multi_transpose, tg, tb, 0, E.stream, dist, n, k, d_dist_out, E.d_cnt + 2);
+  s.reached = (int64_t)E.read_counters()[2].size;
   if (st) *st = s;
 }
 

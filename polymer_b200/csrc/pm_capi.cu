@@ -24,6 +24,8 @@ void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_n
 void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
 void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, int64_t threshold,
                pm_traversal_stats *st);
+void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist, int64_t threshold,
+                  pm_traversal_stats *st);
 void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double damping, float *d_out);
 void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out);
 void generate_er_batch(pm_graph *g, int count, int64_t n_min, int64_t n_max, int avg_degree,
@@ -336,25 +338,48 @@ pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uin
   });
 }
 
+// Checks k and the sources (read back when they live on the device) and
+// stages them in the handle's scratch; returns their device copy.
+static const int32_t *stage_sources(pm_graph *g, const int32_t *sources, int k, uint32_t mem) {
+  need(k >= 1 && k <= 64, "k must be in [1, 64]");
+  int32_t hs[64];
+  if (mem == PM_MEM_DEVICE)
+    PM_CUDA(cudaMemcpy(hs, sources, (size_t)k * 4, cudaMemcpyDeviceToHost));
+  else
+    memcpy(hs, sources, (size_t)k * 4);
+  for (int l = 0; l < k; ++l) need(hs[l] >= 0 && hs[l] < g->n, "source out of range");
+  int32_t *ds = (int32_t *)g->scratch_buf(kSlotIn0, 64 * 4);
+  PM_CUDA(cudaMemcpyAsync(ds, hs, (size_t)k * 4, cudaMemcpyHostToDevice, g->E.stream));
+  return ds;
+}
+
 pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *depth, uint32_t mem,
                        int64_t threshold, pm_traversal_stats *stats) {
   return guard([&] {
     enter(g);
     check_mem(mem);
     need(sources != nullptr && depth != nullptr, "null sources/depth");
-    need(k >= 1 && k <= 64, "k must be in [1, 64]");
-    int32_t hs[64];
-    if (mem == PM_MEM_DEVICE)
-      PM_CUDA(cudaMemcpy(hs, sources, (size_t)k * 4, cudaMemcpyDeviceToHost));
-    else
-      memcpy(hs, sources, (size_t)k * 4);
-    for (int l = 0; l < k; ++l) need(hs[l] >= 0 && hs[l] < g->n, "source out of range");
-    int32_t *ds = (int32_t *)g->scratch_buf(kSlotIn0, 64 * 4);
-    PM_CUDA(cudaMemcpyAsync(ds, hs, (size_t)k * 4, cudaMemcpyHostToDevice, g->E.stream));
+    const int32_t *ds = stage_sources(g, sources, k, mem);
     const size_t bytes = (size_t)g->n * k * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? depth : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
     run_msbfs(g, ds, k, dd, threshold < 0 ? g->m / 20 : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, depth, dd, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dist, uint32_t mem,
+                                int64_t threshold, pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(sources != nullptr && dist != nullptr, "null sources/dist");
+    need(g->w_i32_out.p != nullptr, "graph has no int32 weights (pm_graph_set_weights_i32)");
+    const int32_t *ds = stage_sources(g, sources, k, mem);
+    const size_t bytes = (size_t)g->n * k * 4;
+    int32_t *dd = mem == PM_MEM_DEVICE ? dist : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
+    run_bf_multi(g, ds, k, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    if (mem == PM_MEM_HOST) from_device(g, dist, dd, bytes, mem);
     finish(g);
   });
 }

@@ -46,7 +46,7 @@ def test_weighted_pagerank_matches_oracle(pm, oracle):
 
 @pytest.mark.parametrize("scale,k", [(14, 64), (20, 1024)])
 def test_pagerank_adjoint_vs_fp64_adjoint(pm, oracle, scale, k):
-    """weighted PageRank at scale 20, loss = sum of the ranks of
+    """Weighted PageRank at scale 20, loss = sum of the ranks of
     1024 seeded targets, gradient for every edge weight."""
     og, w = weighted_graph(oracle, scale)
     w64 = w.astype(np.float64)

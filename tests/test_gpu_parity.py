@@ -95,7 +95,7 @@ def test_pagerank_rejects_self_loops(pm):
 
 
 def test_pagerank_config1_f64(pm, oracle):
-    """2^16 vertices, edge factor 16, 10 iterations, FP64."""
+    """2^16 vertices, edge factor 16, 10 iterations, FP64 (the reference's CPU-sized case)."""
     og = oracle.rmat_graph(16, 16)
     ref, res_ref = oracle.pagerank(og, 10, with_resid=True)
     with pm.Graph.rmat(16, 16) as g:
@@ -237,6 +237,42 @@ def test_bellman_ford_exact(pm, oracle, threshold):
             for s in oracle.pick_sources(og, 3):
                 d = pm.BellmanFord(g, int(s), threshold=threshold)
                 assert np.array_equal(d, oracle.dijkstra(og, w, int(s)))
+
+
+def _bf_multi_check(pm, oracle, og, sym, srcs, threshold):
+    w = oracle.weights_int(og)
+    with dev_graph(pm, og, symmetric=sym) as g:
+        g.set_weights(w)
+        dist, st = pm.BellmanFordMulti(srcs, g, threshold=threshold, stats=True)
+    reached = 0
+    for l, s in enumerate(srcs):
+        ref = oracle.dijkstra(og, w, int(s))
+        assert np.array_equal(dist[l], ref), "source %d (lane %d)" % (s, l)
+        reached += (ref < pm.BF_INF).sum()
+    assert st["reached"] == reached
+
+
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+@pytest.mark.parametrize("sym,k", [(True, 64), (False, 64), (True, 5)])
+def test_bellman_ford_multi_matches_dijkstra(pm, oracle, threshold, sym, k):
+    # scale 14 has one row above the heavy-row degree in either direction
+    og = oracle.rmat_graph(14, 16, symmetric=sym)
+    srcs = oracle.pick_sources(og, k, seed=0x5EED0016)
+    if k == 64:
+        srcs[9] = srcs[2]  # a repeated source must give identical rows
+    _bf_multi_check(pm, oracle, og, sym, srcs, threshold)
+
+
+@pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
+def test_bellman_ford_multi_hub(pm, oracle, threshold):
+    # a hub of in-degree 12287 (three heavy chunks, a ragged last piece) on a
+    # ring: lanes fall along the ring and through the hub in the same rounds
+    n = 12288
+    src = np.concatenate([np.arange(1, n), np.zeros(n - 1, np.int64), np.arange(1, n - 1)])
+    dst = np.concatenate([np.zeros(n - 1, np.int64), np.arange(1, n), np.arange(2, n)])
+    og = oracle.graph_from_edges(n, src, dst)
+    srcs = np.array([5, 0, 7000, 12287, 5, 300, 11111], np.int32)
+    _bf_multi_check(pm, oracle, og, False, srcs, threshold)
 
 
 def test_device_weights_match_oracle(pm, oracle):
