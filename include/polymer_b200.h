@@ -291,6 +291,47 @@ PM_API pm_status pm_profile_enable(pm_graph *g, int enable);
 PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_t *passes,
                                  int reset);
 
+/* Run-time tunables of a graph handle.  No counterpart in the reference,
+ * which fixes its load-balance cut-offs at compile time and passes each
+ * application's direction-switch threshold in code (BFS 0, numa-BFS.C:268;
+ * CC m/8, numa-Components.C:226; BellmanFord m/20, numa-BellmanFord.C:182).
+ * Results never depend on them; only speed does. */
+#define PM_TUNE_HEAVY_DEG 0        /* rows with more edges are split in 4096-edge chunks
+                                      (default 2048, range [64, 2^30]) */
+#define PM_TUNE_CTA_EXPAND 1       /* sparse push: CTA-wide expansion from this
+                                      out-degree (default 512) */
+#define PM_TUNE_GRID_EXPAND 2      /* sparse push: grid-wide expansion from this
+                                      out-degree (default 4096) */
+#define PM_TUNE_PULL_CTAS_PER_SM 3 /* resident CTAs per SM of the persistent pulls,
+                                      0 = the occupancy limit (default) */
+#define PM_TUNE_BFS_DIV 4          /* threshold < 0 means m / div: BFS (default 20) */
+#define PM_TUNE_CC_DIV 5           /* ... Components (default 8) */
+#define PM_TUNE_BF_DIV 6           /* ... BellmanFord (default 20) */
+#define PM_TUNE_CUDA_GRAPHS 7      /* 1 (default): the fixed-iteration loops of PageRank,
+                                      SpMV, BP and PPR run as CUDA graphs captured on
+                                      first use and replayed after; 0: plain launches */
+PM_API pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value);
+PM_API pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value);
+
+/* Autotuner: coordinate descent over the tunables application `app` uses
+ * (candidates per tunable, each timed twice after a warm-up on the graph's
+ * stream with CUDA events, a change kept when it saves more than 2 %); the
+ * winners stay set on the handle.  PageRank / SpMV / BP time 3 iterations
+ * (SpMV needs float weights), BFS four fixed sources, CC one run,
+ * BellmanFord one source (needs int32 weights). */
+#define PM_APP_PAGERANK 0
+#define PM_APP_SPMV 1
+#define PM_APP_BP 2
+#define PM_APP_BFS 3
+#define PM_APP_CC 4
+#define PM_APP_BF 5
+typedef struct pm_tune_report {
+  int64_t trials;     /* candidate settings timed                 */
+  double default_ms;  /* time of the settings the handle started with */
+  double best_ms;     /* time of the settings kept                  */
+} pm_tune_report;
+PM_API pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report);
+
 /* Pinned (page-locked) host memory for fast host<->device staging. */
 PM_API pm_status pm_host_alloc(uint64_t bytes, void **out);
 PM_API pm_status pm_host_free(void *p);

@@ -56,6 +56,15 @@ class TraversalStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneReport(C.Structure):
+    _fields_ = [("trials", C.c_int64), ("default_ms", C.c_double), ("best_ms", C.c_double)]
+
+
+# run-time tunables (pm_graph_set_tunable) and applications (pm_tune)
+TUNABLES = {"heavy_deg": 0, "cta_expand": 1, "grid_expand": 2, "pull_ctas_per_sm": 3,
+            "bfs_div": 4, "cc_div": 5, "bf_div": 6, "cuda_graphs": 7}
+APPS = {"pagerank": 0, "spmv": 1, "bp": 2, "bfs": 3, "cc": 4, "bellman_ford": 5}
+
 _lib = None
 
 
@@ -107,6 +116,9 @@ def lib():
         "pm_profile_read": [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(i64), C.c_int],
         "pm_host_alloc": [u64, C.POINTER(vp)],
         "pm_host_free": [vp],
+        "pm_graph_set_tunable": [vp, C.c_int, i64],
+        "pm_graph_get_tunable": [vp, C.c_int, C.POINTER(i64)],
+        "pm_tune": [vp, C.c_int, C.POINTER(TuneReport)],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -274,6 +286,25 @@ class Graph:
         ms, cnt = C.c_double(), C.c_int64()
         _check(lib().pm_profile_read(self._h, tag.encode(), C.byref(ms), C.byref(cnt), int(reset)))
         return ms.value, cnt.value
+
+    def set_tunable(self, name: str, value: int) -> None:
+        _check(lib().pm_graph_set_tunable(self._h, TUNABLES[name], int(value)))
+
+    def get_tunable(self, name: str) -> int:
+        v = C.c_int64()
+        _check(lib().pm_graph_get_tunable(self._h, TUNABLES[name], C.byref(v)))
+        return v.value
+
+    def tunables(self) -> dict:
+        return {k: self.get_tunable(k) for k in TUNABLES}
+
+    def tune(self, app: str) -> dict:
+        """Autotune the tunables `app` uses on this graph; returns the report
+        and the settings kept."""
+        r = TuneReport()
+        _check(lib().pm_tune(self._h, APPS[app], C.byref(r)))
+        return {"trials": r.trials, "default_ms": r.default_ms, "best_ms": r.best_ms,
+                "tunables": self.tunables()}
 
 
 class PinnedArray:

@@ -244,17 +244,20 @@ void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_re
   T *c1 = (T *)g->scratch_buf(3, (size_t)n * sizeof(T));
   PM_LAUNCH((k_pr_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, pc, pn, c0, E.g.out.off, n);
   const T dmp = (T)damping, added = (T)((1.0 - damping) * (1.0 / (double)n));
-  for (int it = 0; it < iters; ++it) {
-    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
-    E.prof.begin("pagerank", E.stream);
-    launch_pull_reduce<int>(E, PR_F<T>{c0, c1, pc, pn, E.g.out.off, dmp, added}, nullptr, nullptr,
-                            E.d_cnt);
-    E.prof.end(E.stream);
-    if (d_resid) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_resid + it);
-    std::swap(pc, pn);
-    std::swap(c0, c1);
-  }
-  PM_CUDA(cudaMemcpyAsync(d_out, pc, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
+  E.run_loop(loop_key("pagerank", (int)sizeof(T), iters, damping, pc, pn, c0, c1, d_resid), [&] {
+    T *a = pc, *b = pn, *x = c0, *y = c1;
+    for (int it = 0; it < iters; ++it) {
+      PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+      E.prof.begin("pagerank", E.stream);
+      launch_pull_reduce<int>(E, PR_F<T>{x, y, a, b, E.g.out.off, dmp, added}, nullptr, nullptr, E.d_cnt);
+      E.prof.end(E.stream);
+      if (d_resid) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_resid + it);
+      std::swap(a, b);
+      std::swap(x, y);
+    }
+  });
+  PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? pn : pc, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice,
+                          E.stream));
 }
 
 // ===========================================================================
@@ -285,15 +288,18 @@ void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_n
   float *y = (float *)g->scratch_buf(1, (size_t)n * 4);
   PM_CUDA(cudaMemcpyAsync(x, d_x0, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
   const float *w_in = g->w_f32_in.as<float>();
-  for (int it = 0; it < iters; ++it) {
-    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
-    E.prof.begin("spmv", E.stream);
-    launch_pull_reduce<float>(E, SPMV_F{x, y}, w_in, nullptr, E.d_cnt);
-    E.prof.end(E.stream);
-    if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
-    std::swap(x, y);
-  }
-  PM_CUDA(cudaMemcpyAsync(d_y, x, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+  E.run_loop(loop_key("spmv", iters, x, y, w_in, d_norm), [&] {
+    float *a = x, *b = y;
+    for (int it = 0; it < iters; ++it) {
+      PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+      E.prof.begin("spmv", E.stream);
+      launch_pull_reduce<float>(E, SPMV_F{a, b}, w_in, nullptr, E.d_cnt);
+      E.prof.end(E.stream);
+      if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
+      std::swap(a, b);
+    }
+  });
+  PM_CUDA(cudaMemcpyAsync(d_y, iters % 2 ? y : x, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
 }
 
 // ===========================================================================
@@ -341,18 +347,23 @@ void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, floa
   PM_CUDA(cudaMemsetAsync(ln, 0, (size_t)n * 8, E.stream));
   VertexSubset cur = g->subset(0), next = g->subset(1);
   subset_all(E, cur);
-  for (int it = 0; it < iters; ++it) {
-    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
-    E.prof.begin("bp", E.stream);
-    launch_pull_reduce<int>(E,
-                            BP_F{cur.bits, lc, ln, (const float2 *)d_prior, psi[0], psi[1], psi[2],
-                                 psi[3]},
-                            nullptr, next.bits, E.d_cnt);
-    E.prof.end(E.stream);
-    std::swap(lc, ln);
-    std::swap(cur, next);
-  }
-  PM_CUDA(cudaMemcpyAsync(d_out, lc, (size_t)n * 8, cudaMemcpyDeviceToDevice, E.stream));
+  E.run_loop(loop_key("bp", iters, lc, ln, cur.bits, next.bits, d_prior, (double)psi[0], (double)psi[1],
+                      (double)psi[2], (double)psi[3]),
+             [&] {
+               float2 *a = lc, *b = ln;
+               uint32_t *fa = cur.bits, *fb = next.bits;
+               for (int it = 0; it < iters; ++it) {
+                 PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+                 E.prof.begin("bp", E.stream);
+                 launch_pull_reduce<int>(
+                     E, BP_F{fa, a, b, (const float2 *)d_prior, psi[0], psi[1], psi[2], psi[3]}, nullptr,
+                     fb, E.d_cnt);
+                 E.prof.end(E.stream);
+                 std::swap(a, b);
+                 std::swap(fa, fb);
+               }
+             });
+  PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? ln : lc, (size_t)n * 8, cudaMemcpyDeviceToDevice, E.stream));
 }
 
 // explicit instantiations used by the C ABI

@@ -304,7 +304,7 @@ __device__ __forceinline__ void bf_multi_relax(const int32_t *__restrict__ in_id
 constexpr int kBfPiece = 512;  // in-edges of one warp's piece of a heavy row
 
 // Dense round.  Persistent warps take tickets: the first ones are 512-edge
-// pieces of the heavy rows (in-degree > kHeavyDeg; they lower the row with
+// pieces of the heavy rows (in-degree > g.heavy_deg; they lower the row with
 // atomicMin and OR the fallen lanes into next_active, which starts at zero),
 // the rest are merge-path row groups whose light rows each warp relaxes in
 // full and whose next_active words it writes.
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) k_bf_multi_pull(GraphView g, const int32_
     const int r0 = __ldg(g.in.gstart + grp), r1 = __ldg(g.in.gstart + grp + 1);
     for (int v = r0; v < r1; ++v) {
       const int e0 = __ldg(g.in.off + v), e1 = __ldg(g.in.off + v + 1);
-      if (e1 - e0 > kHeavyDeg) continue;
+      if (e1 - e0 > g.heavy_deg) continue;
       const int32_t old_lo = dist[(int64_t)v * kLanes + lane];
       const int32_t old_hi = dist[(int64_t)v * kLanes + 32 + lane];
       int32_t lo = old_lo, hi = old_hi;
@@ -420,8 +420,7 @@ void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_
     push_per_sm = std::max(push_per_sm, 1);
   }
   const int64_t heavy_pieces = (int64_t)E.g.in.nchunks * (kChunkEdges / kBfPiece);
-  const int pull_grid = (int)std::max<int64_t>(
-      1, std::min<int64_t>((heavy_pieces + E.g.in.ngroups + 7) / 8, (int64_t)E.num_sms * pull_per_sm));
+  const int pull_grid = E.persistent_grid((heavy_pieces + E.g.in.ngroups + 7) / 8, pull_per_sm);
   const int32_t *w_in = g->w_i32_in.as<int32_t>(), *w_out = g->w_i32_out.as<int32_t>();
   pm_traversal_stats s{};
   E.tag = "bellman_ford_multi";
@@ -469,7 +468,7 @@ void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_
 // each vector's seed).  The contribution matrix C (n x 32 floats, row-major,
 // C[u][j] = x_j[u] / outdeg(u)) is gathered one 128-byte row per in-edge, a
 // full cache line; a warp owns a row and its lanes the 32 columns.  Rows
-// with more than kHeavyDeg in-edges are summed by chunk CTAs first.
+// with more than g.heavy_deg in-edges are summed by chunk CTAs first.
 // ===========================================================================
 constexpr int kPprCols = 32;
 
@@ -529,7 +528,7 @@ __global__ void __launch_bounds__(256) k_ppr_pull(GraphView g, const float *__re
     for (int r = r0; r < r1; ++r) {
       const int64_t o0 = __ldg(g.in.off + r), o1 = __ldg(g.in.off + r + 1);
       float acc;
-      if (o1 - o0 > kHeavyDeg) {
+      if (o1 - o0 > g.heavy_deg) {
         const int first = __ldg(g.in.hfirst + r);
         const int nch = (int)((o1 - o0 + kChunkEdges - 1) / kChunkEdges);
         acc = 0.f;
@@ -570,18 +569,20 @@ void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double dampi
     PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppr_pull, 256, 0));
     if (per_sm < 1) per_sm = 1;
   }
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)E.g.in.ngroups + 7) / 8,
-                                                               (int64_t)E.num_sms * per_sm));
-  for (int it = 0; it < iters; ++it) {
-    PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
-    E.prof.begin("ppr", E.stream);
-    if (E.g.in.nchunks > 0)
-      PM_LAUNCH(k_ppr_heavy, E.g.in.nchunks, 256, 0, E.stream, E.g, c0, part);
-    PM_LAUNCH(k_ppr_pull, grid, 256, 0, E.stream, E.g, c0, c1, it == iters - 1 ? d_out : nullptr, k,
-              part, d_seeds, (float)damping, E.d_cnt);
-    E.prof.end(E.stream);
-    std::swap(c0, c1);
-  }
+  const int grid = E.persistent_grid(((int64_t)E.g.in.ngroups + 7) / 8, per_sm);
+  E.run_loop(loop_key("ppr", iters, k, damping, c0, c1, part, d_seeds, d_out), [&] {
+    float *a = c0, *b = c1;
+    for (int it = 0; it < iters; ++it) {
+      PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
+      E.prof.begin("ppr", E.stream);
+      if (E.g.in.nchunks > 0)
+        PM_LAUNCH(k_ppr_heavy, E.g.in.nchunks, 256, 0, E.stream, E.g, a, part);
+      PM_LAUNCH(k_ppr_pull, grid, 256, 0, E.stream, E.g, a, b, it == iters - 1 ? d_out : nullptr, k, part,
+                d_seeds, (float)damping, E.d_cnt);
+      E.prof.end(E.stream);
+      std::swap(a, b);
+    }
+  });
 }
 
 // ===========================================================================

@@ -38,6 +38,9 @@ int run_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters,
 void run_spmv_backward(pm_graph *g, const float *d_x, const float *d_gy, float *d_dx, float *d_dw);
 void gen_weights_lognormal(pm_graph *g, uint64_t seed);
 void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
+void set_tunable(pm_graph *g, int key, int64_t value);
+int64_t get_tunable(pm_graph *g, int key);
+void tune(pm_graph *g, int app, pm_tune_report *rep);
 }  // namespace pm
 
 using namespace pm;
@@ -331,7 +334,7 @@ pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uin
     const size_t bytes = (size_t)g->n * 4;
     int32_t *dp = (int32_t *)g->scratch_buf(kSlotOut0, bytes);
     int32_t *dd = (int32_t *)g->scratch_buf(kSlotOut1, bytes);
-    run_bfs(g, src, dp, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    run_bfs(g, src, dp, dd, threshold < 0 ? g->m / g->E.tune.bfs_div : threshold, stats);
     if (parents) from_device(g, parents, dp, bytes, mem);
     if (depth) from_device(g, depth, dd, bytes, mem);
     finish(g);
@@ -362,7 +365,7 @@ pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dept
     const int32_t *ds = stage_sources(g, sources, k, mem);
     const size_t bytes = (size_t)g->n * k * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? depth : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_msbfs(g, ds, k, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    run_msbfs(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.bfs_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, depth, dd, bytes, mem);
     finish(g);
   });
@@ -378,7 +381,7 @@ pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int3
     const int32_t *ds = stage_sources(g, sources, k, mem);
     const size_t bytes = (size_t)g->n * k * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? dist : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_bf_multi(g, ds, k, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    run_bf_multi(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.bf_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, dist, dd, bytes, mem);
     finish(g);
   });
@@ -392,7 +395,7 @@ pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t thre
     need(labels != nullptr, "null labels");
     const size_t bytes = (size_t)g->n * 4;
     int32_t *dl = mem == PM_MEM_DEVICE ? labels : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_cc(g, dl, threshold < 0 ? g->m / 8 : threshold, stats);
+    run_cc(g, dl, threshold < 0 ? g->m / g->E.tune.cc_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, labels, dl, bytes, mem);
     finish(g);
   });
@@ -408,7 +411,7 @@ pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem,
     need(g->w_i32_out.p != nullptr, "graph has no int32 weights (pm_graph_set_weights_i32)");
     const size_t bytes = (size_t)g->n * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? dist : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_bellman_ford(g, src, dd, threshold < 0 ? g->m / 20 : threshold, stats);
+    run_bellman_ford(g, src, dd, threshold < 0 ? g->m / g->E.tune.bf_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, dist, dd, bytes, mem);
     finish(g);
   });
@@ -631,18 +634,41 @@ pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_
     enter(g);
     need(tag != nullptr, "null tag");
     finish(g);
+    Profiler &P = g->E.prof;
+    P.fold();
     double tot = 0.0;
     int64_t cnt = 0;
-    for (auto &r : g->E.prof.recs) {
-      if (r.tag != tag) continue;
-      float ms = 0.f;
-      PM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
-      tot += ms;
-      ++cnt;
-    }
+    for (auto &t : P.totals)
+      if (t.tag == tag) {
+        tot = t.ms;
+        cnt = t.passes;
+      }
     if (total_ms) *total_ms = tot;
     if (passes) *passes = cnt;
-    if (reset) g->E.prof.clear();
+    if (reset) P.totals.clear();
+  });
+}
+
+pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value) {
+  return guard([&] {
+    enter(g);
+    set_tunable(g, key, value);
+  });
+}
+
+pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
+  return guard([&] {
+    enter(g);
+    need(value != nullptr, "null value");
+    *value = get_tunable(g, key);
+  });
+}
+
+pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
+  return guard([&] {
+    enter(g);
+    tune(g, app, report);
+    finish(g);
   });
 }
 

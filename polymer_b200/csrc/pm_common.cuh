@@ -21,6 +21,7 @@ struct Failure : std::runtime_error {
 void set_last_error(const std::string &msg);  // text returned by pm_last_error()
 [[noreturn]] void fail_cuda(cudaError_t e, const char *what, const char *file, int line);
 void count_launch(int n = 1);
+long long launches(bool reset);
 
 #define PM_CUDA(call)                                                        \
   do {                                                                       \

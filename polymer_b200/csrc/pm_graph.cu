@@ -121,11 +121,12 @@ __global__ void k_group_starts(const int32_t *off, int64_t n, int32_t G, int32_t
   }
 }
 
-__global__ void k_heavy_counts(const int32_t *off, int64_t n, int32_t *nch, int32_t *maxdeg) {
+__global__ void k_heavy_counts(const int32_t *off, int64_t n, int32_t heavy_deg, int32_t *nch,
+                               int32_t *maxdeg) {
   int32_t md = 0;
   GRID_STRIDE(v, n) {
     int32_t d = off[v + 1] - off[v];
-    nch[v] = d > kHeavyDeg ? (d + kChunkEdges - 1) / kChunkEdges : 0;
+    nch[v] = d > heavy_deg ? (d + kChunkEdges - 1) / kChunkEdges : 0;
     md = max(md, d);
   }
   atomicMax(maxdeg, md);
@@ -206,17 +207,14 @@ __global__ void k_uniform_f32(uint64_t seed, int open, int64_t count, float *x) 
 }
 
 // ---------------------------------------------------------------------------
-static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
-  const int64_t n = g->n, m = g->m;
-  a.ngroups = (int32_t)((m + kRowWork * n + kGroupWork - 1) / kGroupWork);
-  if (a.ngroups < 1) a.ngroups = 1;
-  a.gstart.alloc((size_t)(a.ngroups + 1) * 4);
-  PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), n, a.ngroups,
-            a.gstart.as<int32_t>());
+// Rows with more than heavy_deg edges: chunk counts, their prefix sum
+// (hfirst) and the chunk -> row table (hrow).
+static void build_heavy(pm_graph *g, AdjBuf &a, cudaStream_t st, int32_t heavy_deg) {
+  const int64_t n = g->n;
   DevBuf nch((size_t)(n + 1) * 4), md(4);
   PM_CUDA(cudaMemsetAsync(md.p, 0, 4, st));
   PM_CUDA(cudaMemsetAsync(nch.p, 0, (size_t)(n + 1) * 4, st));
-  PM_LAUNCH(k_heavy_counts, grid1d(n), 256, 0, st, a.off.as<int32_t>(), n, nch.as<int32_t>(),
+  PM_LAUNCH(k_heavy_counts, grid1d(n), 256, 0, st, a.off.as<int32_t>(), n, heavy_deg, nch.as<int32_t>(),
             md.as<int32_t>());
   a.hfirst.alloc((size_t)(n + 1) * 4);
   size_t tmp = 0;
@@ -235,6 +233,43 @@ static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
     PM_LAUNCH(k_heavy_rows, grid1d(n), 256, 0, st, nch.as<int32_t>(), a.hfirst.as<int32_t>(), n,
               a.hrow.as<int32_t>());
   if (&a == &g->out) g->max_out_deg = maxdeg;
+}
+
+static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
+  const int64_t n = g->n, m = g->m;
+  a.ngroups = (int32_t)((m + kRowWork * n + kGroupWork - 1) / kGroupWork);
+  if (a.ngroups < 1) a.ngroups = 1;
+  a.gstart.alloc((size_t)(a.ngroups + 1) * 4);
+  PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), n, a.ngroups,
+            a.gstart.as<int32_t>());
+  build_heavy(g, a, st, g->E.tune.heavy_deg);
+}
+
+// Views of the adjacency and the tunables the kernels read.
+static void set_views(pm_graph *g) {
+  GraphView &v = g->E.g;
+  v.n = (int32_t)g->n;
+  v.m = g->m;
+  v.out = g->out.view();
+  v.in = g->symmetric ? v.out : g->in.view();
+  v.heavy_deg = g->E.tune.heavy_deg;
+  v.cta_expand = g->E.tune.cta_expand;
+  v.grid_expand = g->E.tune.grid_expand;
+}
+
+void apply_tunables(pm_graph *g, int32_t old_heavy_deg) {
+  cudaStream_t st = g->E.stream;
+  g->E.release_graphs();  // captured launches hold the old views
+  if (g->E.tune.heavy_deg != old_heavy_deg) {
+    build_heavy(g, g->out, st, g->E.tune.heavy_deg);
+    if (!g->symmetric) build_heavy(g, g->in, st, g->E.tune.heavy_deg);
+  }
+  set_views(g);
+  const GraphView &v = g->E.g;
+  const size_t pbytes = (size_t)std::max(std::max(v.in.nchunks, v.out.nchunks), 1) * 16;
+  if (g->partials.bytes < pbytes) g->partials.alloc(pbytes);
+  g->E.partials = g->partials.p;
+  PM_CUDA(cudaStreamSynchronize(st));
 }
 
 void finish_graph(pm_graph *g) {
@@ -278,11 +313,8 @@ void finish_graph(pm_graph *g) {
     build_tables(g, g->in, st);
   }
   // Views and workspaces.
-  GraphView &v = g->E.g;
-  v.n = (int32_t)n;
-  v.m = m;
-  v.out = g->out.view();
-  v.in = g->symmetric ? v.out : g->in.view();
+  set_views(g);
+  const GraphView &v = g->E.g;
   const int64_t words = (n + 31) / 32 + 1;
   g->bits0.alloc((size_t)words * 4);
   g->bits1.alloc((size_t)words * 4);
@@ -571,6 +603,7 @@ void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t coun
 
 pm_graph::~pm_graph() {
   if (E.stream) cudaStreamSynchronize(E.stream);
+  E.release_graphs();
   if (h_cnt) cudaFreeHost(h_cnt);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);

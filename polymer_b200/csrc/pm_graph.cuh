@@ -102,6 +102,9 @@ namespace pm {
 // Builds every derived structure (CSC, groups, heavy chunks, workspaces)
 // once out.off / out.idx hold a validated CSR on the device.
 void finish_graph(pm_graph *g);
+// Rebuilds what depends on E.tune (heavy tables when heavy_deg changed from
+// old_heavy_deg, the views, the partials) and drops captured loops.
+void apply_tunables(pm_graph *g, int32_t old_heavy_deg);
 // Writes in_w = out_w[in_eid] (or aliases for symmetric graphs).
 void permute_weights_i32(pm_graph *g);
 void permute_weights_f32(pm_graph *g);

@@ -1,0 +1,217 @@
+// pm_tune.cu -- the autotuner behind pm_tune: coordinate descent over the
+// run-time tunables one application uses, timing each candidate on the
+// graph's own stream with CUDA events and keeping the fastest.
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "pm_graph.cuh"
+
+namespace pm {
+void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
+             pm_traversal_stats *st);
+void run_cc(pm_graph *g, int32_t *d_labels, int64_t threshold, pm_traversal_stats *st);
+void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t threshold,
+                      pm_traversal_stats *st);
+template <class T>
+void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid);
+void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm);
+void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
+void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count);
+
+namespace {
+
+// Scratch slots of the tuner (the algorithms use 0..5, the boundary 8..12).
+enum { kSlotTuneIn = 14, kSlotTuneOut0 = 15, kSlotTuneOut1 = 16 };
+
+int32_t &field(Tunables &t, int key) {
+  switch (key) {
+    case PM_TUNE_HEAVY_DEG: return t.heavy_deg;
+    case PM_TUNE_CTA_EXPAND: return t.cta_expand;
+    case PM_TUNE_GRID_EXPAND: return t.grid_expand;
+    case PM_TUNE_PULL_CTAS_PER_SM: return t.pull_ctas_per_sm;
+    case PM_TUNE_BFS_DIV: return t.bfs_div;
+    case PM_TUNE_CC_DIV: return t.cc_div;
+    case PM_TUNE_BF_DIV: return t.bf_div;
+    case PM_TUNE_CUDA_GRAPHS: return t.cuda_graphs;
+  }
+  fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
+}
+
+// Up to `count` sources with out-edges, spread over the id range by a fixed
+// stride (the same on every call, so trials time the same work).
+std::vector<int32_t> tune_sources(pm_graph *g, int count) {
+  std::vector<int32_t> off(g->n + 1);
+  PM_CUDA(cudaMemcpy(off.data(), g->out.off.p, (size_t)(g->n + 1) * 4, cudaMemcpyDeviceToHost));
+  std::vector<int32_t> src;
+  const int64_t step = std::max<int64_t>(1, g->n / (4 * count + 1));
+  for (int64_t v = step / 2; v < g->n && (int)src.size() < count; v += step)
+    if (off[v + 1] > off[v]) src.push_back((int32_t)v);
+  if (src.empty()) src.push_back(0);
+  return src;
+}
+
+}  // namespace
+
+void set_tunable(pm_graph *g, int key, int64_t value) {
+  Tunables t = g->E.tune;
+  int32_t &f = field(t, key);
+  switch (key) {
+    case PM_TUNE_HEAVY_DEG:
+      if (value < 64 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "heavy_deg must be in [64, 2^30]");
+      break;
+    case PM_TUNE_CTA_EXPAND:
+    case PM_TUNE_GRID_EXPAND:
+      if (value < 32 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "expansion degree must be in [32, 2^30]");
+      break;
+    case PM_TUNE_PULL_CTAS_PER_SM:
+      if (value < 0 || value > 64) fail(PM_ERR_INVALID_ARG, "pull CTAs per SM must be in [0, 64]");
+      break;
+    case PM_TUNE_BFS_DIV:
+    case PM_TUNE_CC_DIV:
+    case PM_TUNE_BF_DIV:
+      if (value < 1 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "threshold divisor must be in [1, 2^30]");
+      break;
+    case PM_TUNE_CUDA_GRAPHS:
+      if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cuda_graphs must be 0 or 1");
+      break;
+  }
+  f = (int32_t)value;
+  const int32_t old_heavy = g->E.tune.heavy_deg;
+  g->E.tune = t;
+  apply_tunables(g, old_heavy);
+}
+
+int64_t get_tunable(pm_graph *g, int key) { return field(g->E.tune, key); }
+
+void tune(pm_graph *g, int app, pm_tune_report *rep) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  std::vector<int> keys;
+  std::function<void()> run;
+  std::vector<int32_t> srcs;
+  const float psi[4] = {0.9f, 0.1f, 0.1f, 0.9f};
+  switch (app) {
+    case PM_APP_PAGERANK: {
+      float *out = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      run = [=] { run_pagerank<float>(g, 3, 0.85, out, nullptr); };
+      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      break;
+    }
+    case PM_APP_SPMV: {
+      if (!g->w_f32_out.p) fail(PM_ERR_INVALID_ARG, "graph has no float weights");
+      float *x = (float *)g->scratch_buf(kSlotTuneIn, (size_t)n * 4);
+      float *y = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      fill_uniform(g, 0x7E57ull, 0, x, n);
+      run = [=] { run_spmv(g, x, 3, y, nullptr); };
+      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      break;
+    }
+    case PM_APP_BP: {
+      float *prior = (float *)g->scratch_buf(kSlotTuneIn, (size_t)n * 8);
+      float *out = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 8);
+      fill_uniform(g, 0x7E58ull, 1, prior, 2 * n);
+      run = [=] { run_bp(g, prior, psi, 3, out); };
+      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      break;
+    }
+    case PM_APP_BFS: {
+      srcs = tune_sources(g, 4);
+      int32_t *p = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      int32_t *d = (int32_t *)g->scratch_buf(kSlotTuneOut1, (size_t)n * 4);
+      run = [=] {
+        for (int32_t s : srcs) run_bfs(g, s, p, d, g->m / g->E.tune.bfs_div, nullptr);
+      };
+      keys = {PM_TUNE_BFS_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG};
+      break;
+    }
+    case PM_APP_CC: {
+      int32_t *l = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      run = [=] { run_cc(g, l, g->m / g->E.tune.cc_div, nullptr); };
+      keys = {PM_TUNE_CC_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
+              PM_TUNE_PULL_CTAS_PER_SM};
+      break;
+    }
+    case PM_APP_BF: {
+      if (!g->w_i32_out.p) fail(PM_ERR_INVALID_ARG, "graph has no int32 weights");
+      srcs = tune_sources(g, 1);
+      int32_t *d = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      run = [=] { run_bellman_ford(g, srcs[0], d, g->m / g->E.tune.bf_div, nullptr); };
+      keys = {PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
+              PM_TUNE_PULL_CTAS_PER_SM};
+      break;
+    }
+    default:
+      fail(PM_ERR_INVALID_ARG, "unknown application " + std::to_string(app));
+  }
+  int occupancy = 1;  // pull CTAs per SM the device allows for the pull kernel
+  {
+    int per_sm = 0;
+    PM_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxBlocksPerMultiprocessor, g->device));
+    occupancy = std::max(1, std::min(per_sm, 8));
+  }
+  cudaEvent_t a, b;
+  PM_CUDA(cudaEventCreate(&a));
+  PM_CUDA(cudaEventCreate(&b));
+  int64_t trials = 0;
+  auto time_once = [&] {
+    run();  // warm-up: first touch, graph capture
+    float best = 1e30f;
+    for (int r = 0; r < 2; ++r) {
+      PM_CUDA(cudaEventRecord(a, E.stream));
+      run();
+      PM_CUDA(cudaEventRecord(b, E.stream));
+      PM_CUDA(cudaEventSynchronize(b));
+      float ms = 0.f;
+      PM_CUDA(cudaEventElapsedTime(&ms, a, b));
+      best = std::min(best, ms);
+    }
+    ++trials;
+    return (double)best;
+  };
+  double best_ms = 0.0, default_ms = 0.0;
+  try {
+    best_ms = default_ms = time_once();
+    for (int key : keys) {
+      std::vector<int64_t> cands;
+      switch (key) {
+        case PM_TUNE_HEAVY_DEG: cands = {1024, 2048, 4096, 8192, 32768}; break;
+        case PM_TUNE_CTA_EXPAND: cands = {128, 256, 512, 1024, 2048}; break;
+        case PM_TUNE_GRID_EXPAND: cands = {2048, 4096, 16384, 65536}; break;
+        case PM_TUNE_PULL_CTAS_PER_SM:
+          cands.push_back(0);
+          for (int c = 1; c < occupancy; ++c) cands.push_back(c);
+          break;
+        case PM_TUNE_BFS_DIV:
+        case PM_TUNE_BF_DIV:
+        case PM_TUNE_CC_DIV: cands = {2, 4, 8, 14, 20, 32, 64, 128}; break;
+      }
+      const int64_t start = get_tunable(g, key);
+      int64_t keep = start;
+      for (int64_t c : cands) {
+        if (c == start) continue;
+        set_tunable(g, key, c);
+        const double ms = time_once();
+        if (ms < best_ms * 0.98) {  // a 2 % margin keeps noise from moving it
+          best_ms = ms;
+          keep = c;
+        }
+      }
+      set_tunable(g, key, keep);
+    }
+  } catch (...) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rep) {
+    rep->trials = trials;
+    rep->default_ms = default_ms;
+    rep->best_ms = best_ms;
+  }
+}
+
+}  // namespace pm

@@ -29,6 +29,7 @@
 //                                                          (edgeMapDenseForward)
 #pragma once
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -38,12 +39,12 @@ namespace pm {
 
 constexpr int kGroupWork = 1024;   // work units (edges + kRowWork per row) of one warp group
 constexpr int kRowWork = 4;       // a row costs about as much as this many edges
-constexpr int kHeavyDeg = 2048;    // rows above this degree are split in chunks
+constexpr int kHeavyDeg = 2048;    // default: rows above this degree are split in chunks
 constexpr int kChunkEdges = 4096;  // edges of one heavy chunk (one CTA)
 constexpr int kChunkThreads = 256;
 constexpr int kPullScan = 32;      // edges a thread scans before deferring a row
-constexpr int kCtaExpand = 512;    // sparse push: CTA-wide expansion above this degree
-constexpr int kGridExpand = 4096;  // sparse push: rows above this degree use the whole grid
+constexpr int kCtaExpand = 512;    // default: sparse push CTA-wide expansion from this degree
+constexpr int kGridExpand = 4096;  // default: sparse push rows from this degree use the whole grid
 constexpr int kMaxHubs = 4096;     // hub rows one sparse round can hand to the grid kernel
 
 // One adjacency direction.
@@ -52,7 +53,7 @@ struct Adj {
   const int32_t *idx = nullptr;     // m
   const int32_t *gstart = nullptr;  // ngroups+1 warp-group row starts (32-aligned; last = n)
   const int32_t *hrow = nullptr;    // heavy chunk -> row
-  const int32_t *hfirst = nullptr;  // row -> its first heavy chunk (rows with deg > kHeavyDeg)
+  const int32_t *hfirst = nullptr;  // row -> its first heavy chunk (rows with deg > heavy_deg)
   int32_t ngroups = 0;
   int32_t nchunks = 0;
 };
@@ -60,6 +61,9 @@ struct Adj {
 struct GraphView {
   int32_t n = 0;
   int64_t m = 0;
+  int32_t heavy_deg = kHeavyDeg;      // rows with more edges than this are chunked
+  int32_t cta_expand = kCtaExpand;    // sparse push degree bins
+  int32_t grid_expand = kGridExpand;
   Adj out;  // CSR
   Adj in;   // CSC (aliases out for symmetric graphs)
 };
@@ -103,7 +107,7 @@ __device__ __forceinline__ void emit_queue(bool act, int d, int32_t *queue, int3
 // Sparse push (edgeMapSparseV3, polymer.h:1928-2003): expand the out-edges of
 // every queued vertex; d joins the next frontier when cond(d) &&
 // updateAtomic(s, d, w) holds and its bit was not yet set this round.
-// Load balance: rows >= kCtaExpand are expanded by the whole CTA, rows >= 32
+// Load balance: rows >= g.cta_expand are expanded by the whole CTA, rows >= 32
 // by one warp, the rest through a CTA-wide scan of their degrees.
 // ---------------------------------------------------------------------------
 template <class F, class W>
@@ -141,7 +145,7 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
         atomicOr(&cnt->err, (unsigned)kErrRange);
       }
       // hub rows go to k_sparse_push_hubs, which spreads them over the grid
-      if (deg >= kGridExpand) {
+      if (deg >= g.grid_expand) {
         unsigned long long slot = atomicAdd(&hub_cnt->size, 1ull);
         if (slot < (unsigned long long)kMaxHubs) {
           hubs[slot] = v;
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
     for (;;) {
       if (tid == 0) s_owner = -1;
       __syncthreads();
-      if (deg >= kCtaExpand) s_owner = tid;
+      if (deg >= g.cta_expand) s_owner = tid;
       __syncthreads();
       int owner = s_owner;
       if (owner < 0) break;
@@ -400,7 +404,7 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
 // flight per lane, folds them locally per row, stores rows that start and
 // end inside it, and hands its first / last partial row to a segmented warp
 // reduction keyed by row.  Row sums collect in shared memory; the row's lane
-// then runs f.commit() (the fused vertexMap).  Rows with more than kHeavyDeg
+// then runs f.commit() (the fused vertexMap).  Rows with more than g.heavy_deg
 // edges are reduced first by k_heavy_reduce (one CTA per kChunkEdges chunk)
 // into partials[], which the owning lane folds in chunk order.  The order of
 // every reduction is fixed, so results are deterministic.
@@ -484,7 +488,7 @@ __global__ void __launch_bounds__(kPullBlock) k_pull_reduce(GraphView g, F f, co
       deg = __ldg(g.in.off + r + 1) - o0;
       live = f.cond(r);
     }
-    const bool heavy = deg > kHeavyDeg;
+    const bool heavy = deg > g.heavy_deg;
     const int ldeg = (live && !heavy) ? deg : 0;
     int total;
     const int pos = warp_excl_scan(ldeg, &total);
@@ -649,7 +653,7 @@ __global__ void __launch_bounds__(256) k_dense_push(GraphView g, const uint32_t 
       o0 = __ldg(g.out.off + r);
       deg = __ldg(g.out.off + r + 1) - o0;
     }
-    const int ldeg = deg > kHeavyDeg ? 0 : deg;
+    const int ldeg = deg > g.heavy_deg ? 0 : deg;
     int total;
     const int pos = warp_excl_scan(ldeg, &total);
     for (int c = 0; c < total; c += 32) {
@@ -786,14 +790,26 @@ struct VertexSubset {
   int64_t words() const { return ((int64_t)n + 31) / 32; }
 };
 
-// CUDA-event brackets around application passes (pm_profile_*).
+// CUDA-event brackets around application passes (pm_profile_*).  Pending
+// brackets are folded into per-tag totals (milliseconds, passes) once the
+// stream has drained.  While a loop is being captured into a CUDA graph the
+// brackets become external event-record nodes owned by that graph; each
+// replay re-records them and fold_graph() adds their times.
 struct Profiler {
   struct Rec {
     std::string tag;
     cudaEvent_t a, b;
   };
+  struct Total {
+    std::string tag;
+    double ms = 0.0;
+    int64_t passes = 0;
+  };
   bool enabled = false;
-  std::vector<Rec> recs;
+  bool capturing = false;
+  std::vector<Rec> recs;          // pending, launched directly
+  std::vector<Rec> captured;      // recorded by the capture in progress
+  std::vector<Total> totals;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t take() {
     if (!pool.empty()) {
@@ -805,27 +821,96 @@ struct Profiler {
     PM_CUDA(cudaEventCreate(&e));
     return e;
   }
+  void record(cudaEvent_t e, cudaStream_t s) {
+    if (capturing)
+      PM_CUDA(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+    else
+      PM_CUDA(cudaEventRecord(e, s));
+  }
   void begin(const char *tag, cudaStream_t s) {
     if (!enabled) return;
     Rec r{tag, take(), take()};
-    PM_CUDA(cudaEventRecord(r.a, s));
-    recs.push_back(r);
+    record(r.a, s);
+    (capturing ? captured : recs).push_back(r);
   }
   void end(cudaStream_t s) {
-    if (!enabled || recs.empty()) return;
-    PM_CUDA(cudaEventRecord(recs.back().b, s));
+    if (!enabled) return;
+    std::vector<Rec> &v = capturing ? captured : recs;
+    if (!v.empty()) record(v.back().b, s);
   }
-  void clear() {
+  void add(const Rec &r) {
+    float ms = 0.f;
+    PM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    for (auto &t : totals)
+      if (t.tag == r.tag) {
+        t.ms += ms;
+        t.passes++;
+        return;
+      }
+    totals.push_back(Total{r.tag, (double)ms, 1});
+  }
+  // The stream has drained: fold the pending brackets.
+  void fold() {
     for (auto &r : recs) {
+      add(r);
       pool.push_back(r.a);
       pool.push_back(r.b);
     }
     recs.clear();
   }
+  void fold_graph(const std::vector<Rec> &g) {
+    for (auto &r : g) add(r);
+  }
+  void release(std::vector<Rec> &v) {
+    for (auto &r : v) {
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    v.clear();
+  }
   ~Profiler() {
-    clear();
+    release(recs);
+    release(captured);
     for (auto e : pool) cudaEventDestroy(e);
   }
+};
+
+// Run-time tunables of one graph (pm_graph_set_tunable, pm_tune).
+struct Tunables {
+  int32_t heavy_deg = kHeavyDeg;     // rows with more edges are split in chunks
+  int32_t cta_expand = kCtaExpand;   // sparse push: CTA-wide expansion from this degree
+  int32_t grid_expand = kGridExpand; // sparse push: grid-wide hub expansion from this degree
+  int32_t pull_ctas_per_sm = 0;      // persistent pull-reduce CTAs per SM (0 = occupancy limit)
+  int32_t bfs_div = 20, cc_div = 8, bf_div = 20;  // default threshold = m / div
+  int32_t cuda_graphs = 1;           // capture the fixed-iteration loops
+};
+
+// Key of a captured loop: its name and every value its launches bake in.
+inline void key_part(std::string &k, const void *p) {
+  char b[24];
+  snprintf(b, sizeof b, "|%p", p);
+  k += b;
+}
+inline void key_part(std::string &k, double x) {
+  uint64_t u;
+  memcpy(&u, &x, 8);
+  k += "|" + std::to_string(u);
+}
+inline void key_part(std::string &k, int64_t x) { k += "|" + std::to_string(x); }
+inline void key_part(std::string &k, int x) { k += "|" + std::to_string(x); }
+template <class... A>
+std::string loop_key(const char *name, A... a) {
+  std::string k(name);
+  (key_part(k, a), ...);
+  return k;
+}
+
+// A captured iteration loop, keyed by everything its launches bake in.
+struct LoopGraph {
+  std::string key;
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;
+  std::vector<Profiler::Rec> recs;
 };
 
 // Per-graph execution context: stream, counters, scratch.
@@ -839,12 +924,20 @@ struct Engine {
   void *partials = nullptr;    // max(in.nchunks, 1) * 16 bytes
   int num_sms = 148;
   Profiler prof;
+  Tunables tune;
+  std::vector<LoopGraph> graphs;  // most recent last
   const char *tag = "edgemap";  // profile tag of the running application
 
   int grid_for(int64_t threads, int block = 256, int per_sm = 8) const {
     int64_t b = (threads + block - 1) / block;
     int64_t cap = (int64_t)num_sms * per_sm;
     return (int)std::max<int64_t>(1, std::min(b, cap));
+  }
+  // CTAs of a persistent kernel: the occupancy limit, or the tuned count.
+  int persistent_grid(int64_t want, int occupancy_per_sm) const {
+    int per_sm = occupancy_per_sm;
+    if (tune.pull_ctas_per_sm > 0) per_sm = std::min(per_sm, tune.pull_ctas_per_sm);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * std::max(per_sm, 1)));
   }
   void reset_counters() {
     PM_CUDA(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(Counters), stream));
@@ -862,6 +955,70 @@ struct Engine {
                  (e & kErrRange ? " (id out of range)" : ""));
       }
     return h_cnt;
+  }
+  void drop_graph(LoopGraph &lg) {
+    if (lg.exec) cudaGraphExecDestroy(lg.exec);
+    lg.exec = nullptr;
+    prof.release(lg.recs);
+  }
+  void release_graphs() {
+    for (auto &lg : graphs) drop_graph(lg);
+    graphs.clear();
+  }
+  // Runs body() -- launches on `stream` only, no host synchronisation --
+  // through a CUDA graph captured the first time `key` is seen (when CUDA
+  // graphs are on), or directly.  The key must name every value the launches
+  // bake in: pointers, sizes, scalars and whether profiling is on.
+  template <class Body>
+  void run_loop(const std::string &key_in, Body &&body) {
+    if (!tune.cuda_graphs) {
+      body();
+      return;
+    }
+    const std::string key = key_in + (prof.enabled ? "|prof" : "|-");
+    LoopGraph *lg = nullptr;
+    for (auto &x : graphs)
+      if (x.key == key) lg = &x;
+    if (!lg) {
+      if (graphs.size() >= 16) {
+        drop_graph(graphs.front());
+        graphs.erase(graphs.begin());
+      }
+      LoopGraph fresh;
+      fresh.key = key;
+      const long long before = launches(false);
+      PM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+      prof.capturing = true;
+      cudaGraph_t cg = nullptr;
+      try {
+        body();
+      } catch (...) {
+        prof.capturing = false;
+        prof.release(prof.captured);
+        cudaStreamEndCapture(stream, &cg);
+        if (cg) cudaGraphDestroy(cg);
+        throw;
+      }
+      prof.capturing = false;
+      fresh.recs.swap(prof.captured);
+      PM_CUDA(cudaStreamEndCapture(stream, &cg));
+      const cudaError_t ie = cudaGraphInstantiate(&fresh.exec, cg, 0);
+      cudaGraphDestroy(cg);
+      if (ie != cudaSuccess) {
+        prof.release(fresh.recs);
+        fail_cuda(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+      }
+      fresh.launches = launches(false) - before;
+      count_launch((int)-fresh.launches);  // captured, not run
+      graphs.push_back(std::move(fresh));
+      lg = &graphs.back();
+    }
+    PM_CUDA(cudaGraphLaunch(lg->exec, stream));
+    count_launch((int)lg->launches);
+    if (prof.enabled && !lg->recs.empty()) {
+      PM_CUDA(cudaStreamSynchronize(stream));
+      prof.fold_graph(lg->recs);
+    }
   }
 };
 
@@ -933,7 +1090,7 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
     if (per_sm < 1) per_sm = 1;
   }
   const int64_t want = ((int64_t)E.g.in.ngroups + kPullBlock / 32 - 1) / (kPullBlock / 32);
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)E.num_sms * per_sm));
+  const int grid = E.persistent_grid(want, per_sm);
   PM_LAUNCH((k_pull_reduce<F, W>), grid, kPullBlock, 0, E.stream, E.g, f, w_in, (const Acc *)partials,
             next_bits, cnt);
 }
