@@ -132,7 +132,8 @@ typedef struct pm_traversal_stats {
  * with BFS_F (numa-BFS.C:59-79): parents[v] = some in-neighbour one level
  * up (parents[src] = src, -1 when unreached); depth[v] = level (or -1).
  * Either output may be NULL.  threshold: direction switch, dense (pull)
- * when |F| + outdeg(F) >= threshold; < 0 selects m/20; 0 forces dense
+ * when |F| + outdeg(F) >= threshold; < 0 selects m / PM_TUNE_BFS_DIV (default
+ * 20); 0 forces dense
  * every level as the reference's BFS does (numa-BFS.C:268). */
 PM_API pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
                  int64_t threshold, pm_traversal_stats *stats);
@@ -151,8 +152,8 @@ PM_API pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_
 /* Connected components by min-label propagation.  Replaces Components(GA)
  * (numa-Components.C:402) with CC_F / CC_Vertex_F (55-119): labels start at
  * the vertex id, every round lowers labels along the out-edges of the
- * frontier (vertices whose label fell).  threshold < 0 selects m/8
- * (numa-Components.C:226). labels: n int32. */
+ * frontier (vertices whose label fell).  threshold < 0 selects m /
+ * PM_TUNE_CC_DIV (default 8, numa-Components.C:226).  labels: n int32. */
 PM_API pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t threshold,
                         pm_traversal_stats *stats);
 
@@ -160,7 +161,8 @@ PM_API pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64
  * (pm_graph_set_weights_i32).  Replaces BF_main(WG, start)
  * (numa-BellmanFord.C:400) with BF_F (61-85): dist starts at 1073741823
  * (INT_MAX/2, 283), dist[src] = 0, a vertex joins the next frontier when
- * its distance falls in the round.  threshold < 0 selects m/20 (182). */
+ * its distance falls in the round.  threshold < 0 selects m /
+ * PM_TUNE_BF_DIV (default 20, numa-BellmanFord.C:182). */
 PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem,
                           int64_t threshold, pm_traversal_stats *stats);
 
@@ -168,7 +170,7 @@ PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32
  * distance lanes per vertex (BF_F of numa-BellmanFord.C:61-85 per lane; the
  * reference runs one source per process).  The frontier is the set of
  * vertices with a lane that fell in the last round; the direction rule of
- * pm_bellman_ford applies to it (threshold < 0 selects m/20).  dist: k*n
+ * pm_bellman_ford applies to it (threshold < 0: m / PM_TUNE_BF_DIV).  dist: k*n
  * int32, source-major (dist[l*n + v] = distance of v from sources[l],
  * 1073741823 when unreached) -- each row equals pm_bellman_ford's dist for
  * that source.  sources: k int32 in mem's space.  stats->reached = number of
@@ -308,8 +310,13 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
 #define PM_TUNE_CC_DIV 5           /* ... Components (default 8) */
 #define PM_TUNE_BF_DIV 6           /* ... BellmanFord (default 20) */
 #define PM_TUNE_CUDA_GRAPHS 7      /* 1 (default): the fixed-iteration loops of PageRank,
-                                      SpMV, BP and PPR run as CUDA graphs captured on
-                                      first use and replayed after; 0: plain launches */
+                                      SpMV, BP and PPR run as CUDA graphs, captured the
+                                      second time a handle runs the same loop (same
+                                      sizes, buffers and scalars) and replayed from
+                                      then on; 0: plain launches */
+/* g == NULL sets / reads the process-wide values that handles created
+ * afterwards start with (so tables that depend on them are built once);
+ * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */
 PM_API pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value);
 PM_API pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value);
 

@@ -137,6 +137,17 @@ def _check(status: int) -> None:
         raise PolymerError(status, lib().pm_last_error().decode(errors="replace"))
 
 
+def set_default_tunable(name: str, value: int) -> None:
+    """Process-wide value of a tunable for graphs created afterwards."""
+    _check(lib().pm_graph_set_tunable(None, TUNABLES[name], int(value)))
+
+
+def get_default_tunable(name: str) -> int:
+    v = C.c_int64()
+    _check(lib().pm_graph_get_tunable(None, TUNABLES[name], C.byref(v)))
+    return v.value
+
+
 def kernel_launches(reset: bool = False) -> int:
     return int(lib().pm_kernel_launches(int(reset)))
 

@@ -39,6 +39,7 @@ void run_spmv_backward(pm_graph *g, const float *d_x, const float *d_gy, float *
 void gen_weights_lognormal(pm_graph *g, uint64_t seed);
 void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
 void set_tunable(pm_graph *g, int key, int64_t value);
+Tunables default_tunables();
 int64_t get_tunable(pm_graph *g, int key);
 void tune(pm_graph *g, int app, pm_tune_report *rep);
 }  // namespace pm
@@ -92,6 +93,7 @@ static pm_graph *new_graph(int device, bool symmetric) {
   auto *g = new pm_graph();
   g->device = device;
   g->symmetric = symmetric;
+  g->E.tune = default_tunables();
   try {
     PM_CUDA(cudaStreamCreateWithFlags(&g->E.stream, cudaStreamNonBlocking));
     PM_CUDA(cudaMallocHost(&g->h_cnt, 3 * sizeof(Counters)));
@@ -651,14 +653,14 @@ pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_
 
 pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value) {
   return guard([&] {
-    enter(g);
+    if (g) enter(g);
     set_tunable(g, key, value);
   });
 }
 
 pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
   return guard([&] {
-    enter(g);
+    if (g) enter(g);
     need(value != nullptr, "null value");
     *value = get_tunable(g, key);
   });

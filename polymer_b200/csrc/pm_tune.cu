@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <vector>
 
 #include "pm_graph.cuh"
@@ -54,9 +55,11 @@ std::vector<int32_t> tune_sources(pm_graph *g, int count) {
 
 }  // namespace
 
-void set_tunable(pm_graph *g, int key, int64_t value) {
-  Tunables t = g->E.tune;
-  int32_t &f = field(t, key);
+namespace {
+std::mutex g_defaults_mu;
+Tunables g_defaults;  // what new handles start with
+
+void check_tunable(int key, int64_t value) {
   switch (key) {
     case PM_TUNE_HEAVY_DEG:
       if (value < 64 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "heavy_deg must be in [64, 2^30]");
@@ -76,14 +79,38 @@ void set_tunable(pm_graph *g, int key, int64_t value) {
     case PM_TUNE_CUDA_GRAPHS:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cuda_graphs must be 0 or 1");
       break;
+    default:
+      fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
   }
-  f = (int32_t)value;
+}
+}  // namespace
+
+Tunables default_tunables() {
+  std::lock_guard<std::mutex> lk(g_defaults_mu);
+  return g_defaults;
+}
+
+void set_tunable(pm_graph *g, int key, int64_t value) {
+  check_tunable(key, value);
+  if (!g) {
+    std::lock_guard<std::mutex> lk(g_defaults_mu);
+    field(g_defaults, key) = (int32_t)value;
+    return;
+  }
+  Tunables t = g->E.tune;
+  field(t, key) = (int32_t)value;
   const int32_t old_heavy = g->E.tune.heavy_deg;
   g->E.tune = t;
   apply_tunables(g, old_heavy);
 }
 
-int64_t get_tunable(pm_graph *g, int key) { return field(g->E.tune, key); }
+int64_t get_tunable(pm_graph *g, int key) {
+  if (!g) {
+    std::lock_guard<std::mutex> lk(g_defaults_mu);
+    return field(g_defaults, key);
+  }
+  return field(g->E.tune, key);
+}
 
 void tune(pm_graph *g, int app, pm_tune_report *rep) {
   Engine &E = g->E;

@@ -908,7 +908,8 @@ std::string loop_key(const char *name, A... a) {
 // A captured iteration loop, keyed by everything its launches bake in.
 struct LoopGraph {
   std::string key;
-  cudaGraphExec_t exec = nullptr;
+  int uses = 0;                    // runs of this loop so far
+  cudaGraphExec_t exec = nullptr;  // captured at the second run
   long long launches = 0;
   std::vector<Profiler::Rec> recs;
 };
@@ -966,9 +967,10 @@ struct Engine {
     graphs.clear();
   }
   // Runs body() -- launches on `stream` only, no host synchronisation --
-  // through a CUDA graph captured the first time `key` is seen (when CUDA
-  // graphs are on), or directly.  The key must name every value the launches
-  // bake in: pointers, sizes, scalars and whether profiling is on.
+  // directly the first time `key` is seen, captured into a CUDA graph the
+  // second time, and by replaying that graph from then on (when CUDA graphs
+  // are on; a loop run once costs no capture).  The key must name every value
+  // the launches bake in: pointers, sizes, scalars and whether profiling is on.
   template <class Body>
   void run_loop(const std::string &key_in, Body &&body) {
     if (!tune.cuda_graphs) {
@@ -984,8 +986,16 @@ struct Engine {
         drop_graph(graphs.front());
         graphs.erase(graphs.begin());
       }
-      LoopGraph fresh;
-      fresh.key = key;
+      graphs.push_back(LoopGraph{});
+      graphs.back().key = key;
+      lg = &graphs.back();
+    }
+    if (++lg->uses == 1) {
+      body();
+      return;
+    }
+    if (!lg->exec) {
+      LoopGraph &fresh = *lg;
       const long long before = launches(false);
       PM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
       prof.capturing = true;
@@ -1010,8 +1020,6 @@ struct Engine {
       }
       fresh.launches = launches(false) - before;
       count_launch((int)-fresh.launches);  // captured, not run
-      graphs.push_back(std::move(fresh));
-      lg = &graphs.back();
     }
     PM_CUDA(cudaGraphLaunch(lg->exec, stream));
     count_launch((int)lg->launches);

@@ -54,3 +54,27 @@ def test_null_handle_is_invalid_arg():
     st = pm.lib().pm_bfs(None, 0, None, None, 0, -1, None)
     assert st == 1
     assert b"null graph" in pm.lib().pm_last_error()
+
+
+def test_default_tunables_host_only():
+    """The process-wide tunables (NULL handle) are host state: set, read back,
+    range-checked and restored without a GPU."""
+    import polymer_b200 as pm
+    defaults = {"heavy_deg": 2048, "cta_expand": 512, "grid_expand": 4096, "pull_ctas_per_sm": 0,
+                "bfs_div": 20, "cc_div": 8, "bf_div": 20, "cuda_graphs": 1}
+    assert {k: pm.get_default_tunable(k) for k in defaults} == defaults
+    try:
+        pm.set_default_tunable("heavy_deg", 4096)
+        pm.set_default_tunable("bfs_div", 64)
+        assert pm.get_default_tunable("heavy_deg") == 4096 and pm.get_default_tunable("bfs_div") == 64
+        for name, bad in (("heavy_deg", 63), ("grid_expand", 31), ("pull_ctas_per_sm", 65),
+                          ("cc_div", 0), ("cuda_graphs", -1)):
+            with pytest.raises(pm.PolymerError) as ei:
+                pm.set_default_tunable(name, bad)
+            assert ei.value.status == 1
+        assert pm.lib().pm_graph_set_tunable(None, 42, 1) == 1
+        assert b"unknown tunable" in pm.lib().pm_last_error()
+    finally:
+        for k, v in defaults.items():
+            pm.set_default_tunable(k, v)
+    assert {k: pm.get_default_tunable(k) for k in defaults} == defaults

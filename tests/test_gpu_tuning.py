@@ -144,3 +144,19 @@ def test_autotuner_keeps_results(pm, oracle, app):
         elif app == "bellman_ford":
             s = int(oracle.pick_sources(og, 1)[0])
             assert np.array_equal(pm.BellmanFord(g, s), oracle.dijkstra(og, w, s))
+
+
+def test_defaults_apply_to_new_graphs(pm, oracle):
+    og = oracle.rmat_graph(14, 16)
+    ref = oracle.pagerank(og, 10)
+    try:
+        pm.set_default_tunable("heavy_deg", 256)
+        pm.set_default_tunable("cuda_graphs", 0)
+        with pm.Graph.from_csr(og.off, og.idx) as g:
+            assert g.get_tunable("heavy_deg") == 256 and g.get_tunable("cuda_graphs") == 0
+            assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
+    finally:
+        pm.set_default_tunable("heavy_deg", 2048)
+        pm.set_default_tunable("cuda_graphs", 1)
+    with pm.Graph.from_csr(og.off, og.idx) as g:
+        assert g.get_tunable("heavy_deg") == 2048
