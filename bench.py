@@ -219,6 +219,34 @@ class Suite:
         return total_ms, total_edges
 
 
+def errors_block(pm, suite):
+    """FP32 results of the timed suite against the same computations in FP64
+    on the same graph and inputs (pm_pagerank PM_F64, pm_spmv_f64, pm_bp_f64,
+    which the tests pin to the FP64 oracle): max-abs and relative-L1 error per
+    result, computed on the device in FP64."""
+    torch, B = suite.torch, suite.B
+
+    def err(a32, a64):
+        a = a32.reshape(-1).to(torch.float64)
+        b = a64.reshape(-1)
+        d = (a - b).abs()
+        return {"max_abs": float(d.max()), "max_abs_fp64_value": float(b.abs().max()),
+                "rel_l1": float(d.sum() / b.abs().sum().clamp_min(1e-300))}
+
+    out = {}
+    r32 = pm.PageRank(B, 20, dtype=np.float32, device_out=suite.outB)
+    r64 = pm.PageRank(B, 20, dtype=np.float64, device_out=suite.outB)
+    out["pagerank_20it"] = err(r32, r64)
+    y32 = pm.SPMV(B, suite.x0, 10)
+    y64 = pm.SPMV(B, suite.x0, 10, dtype=np.float64)
+    out["spmv_10it"] = err(y32, y64)
+    l32 = pm.BeliefPropagation(B, suite.prior, 10)
+    l64 = pm.BeliefPropagation(B, suite.prior, 10, dtype=np.float64)
+    out["bp_10it_logprod"] = err(l32, l64)
+    out["reference_precision"] = "FP64 on the GPU, same graph and inputs (tests pin it to the FP64 oracle)"
+    return out
+
+
 def use_tunables(pm, like):
     """Make `like`'s tunables the defaults of graphs created from now on (a
     user who tuned once stores the settings with the workload)."""
@@ -683,6 +711,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline()
         except Exception as exc:  # keep the GPU line even if the CPU sample fails
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    line["errors_vs_fp64"] = errors_block(pm, suite)
     if not args.no_batched:
         line["batched"] = batched_block(pm, suite)
         line["adjoint"] = adjoint_block(pm, torch, suite.dev)

@@ -213,6 +213,12 @@ PM_API pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, dou
  * floats. norm1 (optional, iters doubles): FP64 L1 norm of each y. */
 PM_API pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem,
                   double *norm1);
+/* pm_spmv with FP64 vectors and FP64 sums (the float weights are widened):
+ * the same iteration in the reference's own precision (numa-SPMV.C keeps
+ * double values), the yardstick against which the FP32 result's max-abs and
+ * relative-L1 errors are measured at full size.  x0, y: n doubles. */
+PM_API pm_status pm_spmv_f64(pm_graph *g, const double *x0, int iters, double *y, uint32_t mem,
+                             double *norm1);
 
 /* ---- Differentiation (no reference counterpart; weighted forms of SPMV_F,
  * numa-SPMV.C:72-81, with PR_Vertex_F's damping, numa-PageRank.C:125-137).
@@ -256,6 +262,10 @@ PM_API pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed);
  * edges. */
 PM_API pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
                 uint32_t mem);
+/* pm_bp in FP64 (prior n x 2, psi 4, log_prod n x 2 doubles; device arrays
+ * 16-byte aligned): the yardstick for the FP32 result's error. */
+PM_API pm_status pm_bp_f64(pm_graph *g, const double *prior, const double *psi, int iters,
+                           double *log_prod, uint32_t mem);
 
 /* PageRank for callers that cannot allocate GPU memory.  No counterpart in
  * the reference.  Some hosts may not call cudaMalloc while they run (a

@@ -109,7 +109,9 @@ def lib():
         "pm_bellman_ford": [vp, i32, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_pagerank": [vp, C.c_int, C.c_double, C.c_int, vp, u32, vp],
         "pm_spmv": [vp, vp, C.c_int, vp, u32, vp],
+        "pm_spmv_f64": [vp, vp, C.c_int, vp, u32, vp],
         "pm_bp": [vp, vp, vp, C.c_int, vp, u32],
+        "pm_bp_f64": [vp, vp, vp, C.c_int, vp, u32],
         "pm_timer_begin": [vp],
         "pm_timer_end": [vp, C.POINTER(C.c_float)],
         "pm_profile_enable": [vp, C.c_int],
@@ -517,34 +519,50 @@ def PersonalizedPageRank(g: Graph, seeds, maxIter: int = 20, damping: float = 0.
     return res.reshape(g.n, k)
 
 
-def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False, out=None):
-    """x <- A_w^T x, maxIter times, over the float weights (numa-SPMV.C SPMV_F)."""
-    px, mem, keep = _arg(x0, np.float32)
-    y, py, mem2 = _out(x0 if mem == PM_MEM_DEVICE else None, g.n, np.float32, out)
+def _arg_typed(a, dtype):
+    """_arg with device tensors converted to dtype when they differ."""
+    if a is not None and _is_device(a):
+        import torch
+        want = {np.float32: torch.float32, np.float64: torch.float64}[dtype]
+        if a.dtype != want:
+            a = a.to(want).contiguous()
+    return _arg(a, dtype)
+
+
+def SPMV(g: Graph, x0, maxIter: int = 10, norms: bool = False, out=None, dtype=np.float32):
+    """x <- A_w^T x, maxIter times, over the float weights (numa-SPMV.C SPMV_F);
+    dtype float32 (FP32 vectors and sums) or float64 (the FP64 yardstick)."""
+    dt = np.float64 if np.dtype(dtype) == np.float64 else np.float32
+    px, mem, keep = _arg_typed(x0, dt)
+    y, py, mem2 = _out(keep if mem == PM_MEM_DEVICE else None, g.n, dt, out)
     if mem != mem2:
         raise PolymerError(1, "x0 and out must live in the same memory space")
     nrm = np.zeros(max(maxIter, 1), np.float64)
-    _check(lib().pm_spmv(g.handle, px, int(maxIter), py, mem,
-                         nrm.ctypes.data_as(C.c_void_p) if norms else None))
+    fn = lib().pm_spmv_f64 if dt == np.float64 else lib().pm_spmv
+    _check(fn(g.handle, px, int(maxIter), py, mem, nrm.ctypes.data_as(C.c_void_p) if norms else None))
     return (y, nrm[:maxIter]) if norms else y
 
 
-def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1, 0.9)), out=None):
-    """2-state BP log-products (n x 2) (numa-BP.C BP_F, normalised messages)."""
-    pp, mem, keep = _arg(prior, np.float32)
-    psi_a = np.ascontiguousarray(psi, np.float32).reshape(4)
+def BeliefPropagation(g: Graph, prior, maxIter: int = 10, psi=((0.9, 0.1), (0.1, 0.9)), out=None,
+                      dtype=np.float32):
+    """2-state BP log-products (n x 2) (numa-BP.C BP_F, normalised messages);
+    dtype float32 or float64."""
+    dt = np.float64 if np.dtype(dtype) == np.float64 else np.float32
+    pp, mem, keep = _arg_typed(prior, dt)
+    psi_a = np.ascontiguousarray(psi, dt).reshape(4)
     if mem == PM_MEM_DEVICE:
         import torch
-        psi_t = torch.tensor(psi_a, device=prior.device)
+        psi_t = torch.tensor(psi_a, device=keep.device)
         ppsi = C.c_void_p(psi_t.data_ptr())
     else:
         psi_t = psi_a
         ppsi = psi_a.ctypes.data_as(C.c_void_p)
     flat = None if out is None else out.reshape(-1)
-    res, po, mem2 = _out(prior if mem == PM_MEM_DEVICE else None, 2 * g.n, np.float32, flat)
+    res, po, mem2 = _out(keep if mem == PM_MEM_DEVICE else None, 2 * g.n, dt, flat)
     if mem != mem2:
         raise PolymerError(1, "prior and out must live in the same memory space")
-    _check(lib().pm_bp(g.handle, pp, ppsi, int(maxIter), po, mem))
+    fn = lib().pm_bp_f64 if dt == np.float64 else lib().pm_bp
+    _check(fn(g.handle, pp, ppsi, int(maxIter), po, mem))
     return res.reshape(g.n, 2)
 
 

@@ -265,41 +265,45 @@ void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_re
 // All vertices are active every iteration: y[d] = sum w(s,d) x[s] as a
 // pull over the CSC with the weights permuted to CSC order; x <- y.
 // ===========================================================================
+template <class T>
 struct SPMV_F {
-  const float *x;
-  float *y;
-  using Acc = float;
+  const T *x;
+  T *y;
+  using Acc = T;
   __device__ __forceinline__ bool cond(int) const { return true; }
-  __device__ __forceinline__ Acc identity() const { return -0.0f; }
-  __device__ __forceinline__ Acc edge(int s, int, float w) const { return w * __ldg(x + s); }
+  __device__ __forceinline__ Acc identity() const { return T(-0.0); }
+  __device__ __forceinline__ Acc edge(int s, int, float w) const { return T(w) * __ldg(x + s); }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
   __device__ __forceinline__ bool commit(int d, Acc acc, double2 &norm) const {
-    const float v = acc + 0.0f;
+    const T v = acc + T(0);
     y[d] = v;
     norm.x += fabs((double)v);
     return false;
   }
 };
 
-void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm) {
+// T = float: the FP32 storage and sums of the benchmark; T = double: the same
+// iteration in FP64, the yardstick for the FP32 result's error.
+template <class T>
+void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm) {
   Engine &E = g->E;
   const int64_t n = g->n;
-  float *x = (float *)g->scratch_buf(0, (size_t)n * 4);
-  float *y = (float *)g->scratch_buf(1, (size_t)n * 4);
-  PM_CUDA(cudaMemcpyAsync(x, d_x0, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+  T *x = (T *)g->scratch_buf(0, (size_t)n * sizeof(T));
+  T *y = (T *)g->scratch_buf(1, (size_t)n * sizeof(T));
+  PM_CUDA(cudaMemcpyAsync(x, d_x0, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
   const float *w_in = g->w_f32_in.as<float>();
-  E.run_loop(loop_key("spmv", iters, x, y, w_in, d_norm), [&] {
-    float *a = x, *b = y;
+  E.run_loop(loop_key("spmv", (int)sizeof(T), iters, x, y, w_in, d_norm), [&] {
+    T *a = x, *b = y;
     for (int it = 0; it < iters; ++it) {
       PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
       E.prof.begin("spmv", E.stream);
-      launch_pull_reduce<float>(E, SPMV_F{a, b}, w_in, nullptr, E.d_cnt);
+      launch_pull_reduce<float>(E, SPMV_F<T>{a, b}, w_in, nullptr, E.d_cnt);
       E.prof.end(E.stream);
       if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
       std::swap(a, b);
     }
   });
-  PM_CUDA(cudaMemcpyAsync(d_y, iters % 2 ? y : x, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+  PM_CUDA(cudaMemcpyAsync(d_y, iters % 2 ? y : x, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
 }
 
 // ===========================================================================
@@ -310,12 +314,22 @@ void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_n
 // the frontier: the pull reduces k_d and commit() applies it, in logs.
 // Messages are normalised to sum 1 (see pm_bp in the header).
 // ===========================================================================
+template <class T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+__device__ __forceinline__ float bp_exp(float x) { return expf(x); }
+__device__ __forceinline__ double bp_exp(double x) { return exp(x); }
+__device__ __forceinline__ float bp_log(float x) { return logf(x); }
+__device__ __forceinline__ double bp_log(double x) { return log(x); }
+
+template <class T>
 struct BP_F {
+  using V = typename Vec2<T>::type;
   const uint32_t *cur;
-  const float2 *lc;
-  float2 *ln;
-  const float2 *prior;
-  float p00, p01, p10, p11;
+  const V *lc;
+  V *ln;
+  const V *prior;
+  T p00, p01, p10, p11;
   using Acc = int32_t;
   __device__ __forceinline__ bool cond(int) const { return true; }
   __device__ __forceinline__ Acc identity() const { return 0; }
@@ -323,51 +337,62 @@ struct BP_F {
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
   __device__ __forceinline__ bool commit(int d, Acc k, double2 &) const {
     const bool in_f = test_bit(cur, d);
-    float2 out = in_f ? make_float2(0.f, 0.f) : ln[d];
+    V out;
+    if (in_f)
+      out.x = out.y = T(0);
+    else
+      out = ln[d];
     if (k > 0) {
-      const float2 l = lc[d], pr = prior[d];
-      const float lm = fmaxf(l.x, l.y);
-      const float a0 = pr.x * expf(l.x - lm), a1 = pr.y * expf(l.y - lm);
-      const float b0 = p00 * a0 + p01 * a1, b1 = p10 * a0 + p11 * a1;
-      const float lz = logf(b0 + b1);
-      out.x += (float)k * (logf(b0) - lz);
-      out.y += (float)k * (logf(b1) - lz);
+      const V l = lc[d], pr = prior[d];
+      const T lm = l.x > l.y ? l.x : l.y;
+      const T a0 = pr.x * bp_exp(l.x - lm), a1 = pr.y * bp_exp(l.y - lm);
+      const T b0 = p00 * a0 + p01 * a1, b1 = p10 * a0 + p11 * a1;
+      const T lz = bp_log(b0 + b1);
+      out.x += (T)k * (bp_log(b0) - lz);
+      out.y += (T)k * (bp_log(b1) - lz);
     }
     if (in_f || k > 0) ln[d] = out;
     return k > 0;
   }
 };
 
-void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out) {
+template <class T>
+void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out) {
+  using V = typename Vec2<T>::type;
   Engine &E = g->E;
   const int64_t n = g->n;
-  float2 *lc = (float2 *)g->scratch_buf(0, (size_t)n * 8);
-  float2 *ln = (float2 *)g->scratch_buf(1, (size_t)n * 8);
-  PM_CUDA(cudaMemsetAsync(lc, 0, (size_t)n * 8, E.stream));
-  PM_CUDA(cudaMemsetAsync(ln, 0, (size_t)n * 8, E.stream));
+  V *lc = (V *)g->scratch_buf(0, (size_t)n * sizeof(V));
+  V *ln = (V *)g->scratch_buf(1, (size_t)n * sizeof(V));
+  PM_CUDA(cudaMemsetAsync(lc, 0, (size_t)n * sizeof(V), E.stream));
+  PM_CUDA(cudaMemsetAsync(ln, 0, (size_t)n * sizeof(V), E.stream));
   VertexSubset cur = g->subset(0), next = g->subset(1);
   subset_all(E, cur);
-  E.run_loop(loop_key("bp", iters, lc, ln, cur.bits, next.bits, d_prior, (double)psi[0], (double)psi[1],
-                      (double)psi[2], (double)psi[3]),
+  E.run_loop(loop_key("bp", (int)sizeof(T), iters, lc, ln, cur.bits, next.bits, d_prior, (double)psi[0],
+                      (double)psi[1], (double)psi[2], (double)psi[3]),
              [&] {
-               float2 *a = lc, *b = ln;
+               V *a = lc, *b = ln;
                uint32_t *fa = cur.bits, *fb = next.bits;
                for (int it = 0; it < iters; ++it) {
                  PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
                  E.prof.begin("bp", E.stream);
                  launch_pull_reduce<int>(
-                     E, BP_F{fa, a, b, (const float2 *)d_prior, psi[0], psi[1], psi[2], psi[3]}, nullptr,
+                     E, BP_F<T>{fa, a, b, (const V *)d_prior, psi[0], psi[1], psi[2], psi[3]}, nullptr,
                      fb, E.d_cnt);
                  E.prof.end(E.stream);
                  std::swap(a, b);
                  std::swap(fa, fb);
                }
              });
-  PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? ln : lc, (size_t)n * 8, cudaMemcpyDeviceToDevice, E.stream));
+  PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? ln : lc, (size_t)n * sizeof(V), cudaMemcpyDeviceToDevice,
+                          E.stream));
 }
 
 // explicit instantiations used by the C ABI
 template void run_pagerank<float>(pm_graph *, int, double, float *, double *);
 template void run_pagerank<double>(pm_graph *, int, double, double *, double *);
+template void run_spmv<float>(pm_graph *, const float *, int, float *, double *);
+template void run_spmv<double>(pm_graph *, const double *, int, double *, double *);
+template void run_bp<float>(pm_graph *, const float *, const float *, int, float *);
+template void run_bp<double>(pm_graph *, const double *, const double *, int, double *);
 
 }  // namespace pm

@@ -20,8 +20,10 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
                       pm_traversal_stats *st);
 template <class T>
 void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid);
-void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm);
-void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
+template <class T>
+void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm);
+template <class T>
+void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out);
 void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, int64_t threshold,
                pm_traversal_stats *st);
 void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist, int64_t threshold,
@@ -469,27 +471,36 @@ pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, double dam
   });
 }
 
+extern "C++" {
+template <class T>
+static void spmv_call(pm_graph *g, const T *x0, int iters, T *y, uint32_t mem, double *norm1) {
+  enter(g);
+  check_mem(mem);
+  need(x0 != nullptr && y != nullptr, "null x0/y");
+  need(iters >= 0, "iters must be >= 0");
+  need(g->w_f32_out.p != nullptr, "graph has no float weights (pm_graph_set_weights_f32)");
+  const size_t bytes = (size_t)g->n * sizeof(T);
+  const T *dx = x0;
+  if (mem == PM_MEM_HOST) {
+    T *t = (T *)g->scratch_buf(kSlotIn0, bytes);
+    to_device(g, t, x0, bytes, mem);
+    dx = t;
+  }
+  T *dy = mem == PM_MEM_DEVICE ? y : (T *)g->scratch_buf(kSlotOut0, bytes);
+  double *dn = norm1 ? (double *)g->scratch_buf(kSlotAux, (size_t)std::max(iters, 1) * 8) : nullptr;
+  run_spmv<T>(g, dx, iters, dy, dn);
+  if (mem == PM_MEM_HOST) from_device(g, y, dy, bytes, mem);
+  if (norm1 && iters > 0) from_device(g, norm1, dn, (size_t)iters * 8, PM_MEM_HOST);
+  finish(g);
+}
+}  // extern "C++"
+
 pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem, double *norm1) {
-  return guard([&] {
-    enter(g);
-    check_mem(mem);
-    need(x0 != nullptr && y != nullptr, "null x0/y");
-    need(iters >= 0, "iters must be >= 0");
-    need(g->w_f32_out.p != nullptr, "graph has no float weights (pm_graph_set_weights_f32)");
-    const size_t bytes = (size_t)g->n * 4;
-    const float *dx = x0;
-    if (mem == PM_MEM_HOST) {
-      float *t = (float *)g->scratch_buf(kSlotIn0, bytes);
-      to_device(g, t, x0, bytes, mem);
-      dx = t;
-    }
-    float *dy = mem == PM_MEM_DEVICE ? y : (float *)g->scratch_buf(kSlotOut0, bytes);
-    double *dn = norm1 ? (double *)g->scratch_buf(kSlotAux, (size_t)std::max(iters, 1) * 8) : nullptr;
-    run_spmv(g, dx, iters, dy, dn);
-    if (mem == PM_MEM_HOST) from_device(g, y, dy, bytes, mem);
-    if (norm1 && iters > 0) from_device(g, norm1, dn, (size_t)iters * 8, PM_MEM_HOST);
-    finish(g);
-  });
+  return guard([&] { spmv_call<float>(g, x0, iters, y, mem, norm1); });
+}
+
+pm_status pm_spmv_f64(pm_graph *g, const double *x0, int iters, double *y, uint32_t mem, double *norm1) {
+  return guard([&] { spmv_call<double>(g, x0, iters, y, mem, norm1); });
 }
 
 static void need_weights_f32(pm_graph *g) {
@@ -575,34 +586,46 @@ pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed) {
   });
 }
 
+extern "C++" {
+template <class T>
+static void bp_call(pm_graph *g, const T *prior, const T *psi, int iters, T *log_prod, uint32_t mem) {
+  enter(g);
+  check_mem(mem);
+  need(prior != nullptr && psi != nullptr && log_prod != nullptr, "null prior/psi/log_prod");
+  need(iters >= 0, "iters must be >= 0");
+  const uintptr_t align = 2 * sizeof(T) - 1;
+  need(mem == PM_MEM_HOST || (((uintptr_t)prior | (uintptr_t)log_prod) & align) == 0,
+       sizeof(T) == 4 ? "device prior/log_prod must be 8-byte aligned"
+                      : "device prior/log_prod must be 16-byte aligned");
+  const size_t bytes = (size_t)g->n * 2 * sizeof(T);
+  T hpsi[4];
+  if (mem == PM_MEM_DEVICE) {
+    PM_CUDA(cudaMemcpy(hpsi, psi, sizeof hpsi, cudaMemcpyDeviceToHost));
+  } else {
+    memcpy(hpsi, psi, sizeof hpsi);
+  }
+  for (T p : hpsi) need(p > T(0) && std::isfinite(p), "psi entries must be positive and finite");
+  const T *dp = prior;
+  if (mem == PM_MEM_HOST) {
+    T *t = (T *)g->scratch_buf(kSlotIn0, bytes);
+    to_device(g, t, prior, bytes, mem);
+    dp = t;
+  }
+  T *dout = mem == PM_MEM_DEVICE ? log_prod : (T *)g->scratch_buf(kSlotOut0, bytes);
+  run_bp<T>(g, dp, hpsi, iters, dout);
+  if (mem == PM_MEM_HOST) from_device(g, log_prod, dout, bytes, mem);
+  finish(g);
+}
+}  // extern "C++"
+
 pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
                 uint32_t mem) {
-  return guard([&] {
-    enter(g);
-    check_mem(mem);
-    need(prior != nullptr && psi != nullptr && log_prod != nullptr, "null prior/psi/log_prod");
-    need(iters >= 0, "iters must be >= 0");
-    need(mem == PM_MEM_HOST || (((uintptr_t)prior | (uintptr_t)log_prod) & 7) == 0,
-         "device prior/log_prod must be 8-byte aligned");
-    const size_t bytes = (size_t)g->n * 8;
-    float hpsi[4];
-    if (mem == PM_MEM_DEVICE) {
-      PM_CUDA(cudaMemcpy(hpsi, psi, sizeof hpsi, cudaMemcpyDeviceToHost));
-    } else {
-      memcpy(hpsi, psi, sizeof hpsi);
-    }
-    for (float p : hpsi) need(p > 0.0f && std::isfinite(p), "psi entries must be positive and finite");
-    const float *dp = prior;
-    if (mem == PM_MEM_HOST) {
-      float *t = (float *)g->scratch_buf(kSlotIn0, bytes);
-      to_device(g, t, prior, bytes, mem);
-      dp = t;
-    }
-    float *dout = mem == PM_MEM_DEVICE ? log_prod : (float *)g->scratch_buf(kSlotOut0, bytes);
-    run_bp(g, dp, hpsi, iters, dout);
-    if (mem == PM_MEM_HOST) from_device(g, log_prod, dout, bytes, mem);
-    finish(g);
-  });
+  return guard([&] { bp_call<float>(g, prior, psi, iters, log_prod, mem); });
+}
+
+pm_status pm_bp_f64(pm_graph *g, const double *prior, const double *psi, int iters, double *log_prod,
+                    uint32_t mem) {
+  return guard([&] { bp_call<double>(g, prior, psi, iters, log_prod, mem); });
 }
 
 pm_status pm_timer_begin(pm_graph *g) {

@@ -17,8 +17,10 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
                       pm_traversal_stats *st);
 template <class T>
 void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid);
-void run_spmv(pm_graph *g, const float *d_x0, int iters, float *d_y, double *d_norm);
-void run_bp(pm_graph *g, const float *d_prior, const float *psi, int iters, float *d_out);
+template <class T>
+void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm);
+template <class T>
+void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out);
 void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count);
 
 namespace {

@@ -306,6 +306,28 @@ def test_spmv_f32_rel_l1(pm, oracle):
     assert abs(norms[-1] / np.abs(ref).sum() - 1) < RL1_F32
 
 
+def test_spmv_f64_matches_oracle_and_reference(pm, oracle):
+    """FP64 vectors and sums: elementwise against the FP64 oracle, and against
+    the reference's printed output (%.9e) on its integer-weight fixture."""
+    og = oracle.rmat_graph(16, 16)
+    w = oracle.weights_unit(og)
+    x0 = oracle.uniform01(og.n)
+    ref = oracle.spmv(og, w.astype(np.float64), x0.astype(np.float64), 10)
+    with dev_graph(pm, og) as g:
+        g.set_weights(w)
+        y, norms = pm.SPMV(g, x0.astype(np.float64), 10, norms=True, dtype=np.float64)
+        y32 = pm.SPMV(g, x0, 10)
+    assert y.dtype == np.float64 and np.allclose(y, ref, rtol=RTOL_F64, atol=0)
+    assert abs(norms[-1] / np.abs(ref).sum() - 1) < 1e-12
+    assert rel_l1(y32, y) < RL1_F32
+    z = load("rmat10_directed.npz")
+    n = len(z["off"]) - 1
+    with pm.Graph.from_csr(z["off"], z["idx"]) as g:
+        g.set_weights(z["spmv_w"].astype(np.float32))
+        y = pm.SPMV(g, np.full(n, 1.0 / n), 5, dtype=np.float64)
+    assert np.allclose(y, z["spmv5"], rtol=2e-9, atol=0)
+
+
 # --------------------------------------------------------------------------
 @pytest.mark.parametrize("k", [32, 3])
 def test_ppr_matches_oracle(pm, oracle, k):
@@ -372,6 +394,19 @@ def test_bp_matches_oracle(pm, oracle):
         out = pm.BeliefPropagation(g, prior, 10)
     err = np.abs(out - ref).sum() / max(np.abs(ref).sum(), 1e-30)
     assert err < RL1_F32, err
+
+
+def test_bp_f64_matches_oracle(pm, oracle):
+    og = oracle.rmat_graph(14, 16)
+    prior = oracle.uniform_open(2 * og.n).reshape(og.n, 2).astype(np.float64)
+    ref = oracle.bp(og, prior, 10)
+    with dev_graph(pm, og) as g:
+        out = pm.BeliefPropagation(g, prior, 10, dtype=np.float64)
+        out_dev = pm.BeliefPropagation(g, __import__("torch").from_numpy(prior).cuda(), 10,
+                                       dtype=np.float64)
+    assert out.dtype == np.float64
+    assert np.allclose(out, ref, rtol=1e-9, atol=1e-12)
+    assert np.array_equal(out_dev.cpu().numpy(), out)
 
 
 # --------------------------------------------------------------------------
