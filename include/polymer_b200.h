@@ -348,6 +348,12 @@ typedef struct pm_tune_report {
   double best_ms;     /* time of the settings kept                  */
 } pm_tune_report;
 PM_API pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report);
+/* The same over a mix of applications that share the handle (count <= 6):
+ * the objective is their summed time, the tunables are the union of theirs,
+ * and the descent sweeps them twice when the first sweep moved one -- the
+ * shared cut-offs are then chosen for the mix, not for whichever application
+ * was tuned last. */
+PM_API pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report);
 
 /* Pinned (page-locked) host memory for fast host<->device staging. */
 PM_API pm_status pm_host_alloc(uint64_t bytes, void **out);

@@ -121,6 +121,7 @@ def lib():
         "pm_graph_set_tunable": [vp, C.c_int, i64],
         "pm_graph_get_tunable": [vp, C.c_int, C.POINTER(i64)],
         "pm_tune": [vp, C.c_int, C.POINTER(TuneReport)],
+        "pm_tune_mix": [vp, vp, C.c_int, C.POINTER(TuneReport)],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -311,11 +312,15 @@ class Graph:
     def tunables(self) -> dict:
         return {k: self.get_tunable(k) for k in TUNABLES}
 
-    def tune(self, app: str) -> dict:
-        """Autotune the tunables `app` uses on this graph; returns the report
-        and the settings kept."""
+    def tune(self, app) -> dict:
+        """Autotune the tunables `app` (a name, or a list of names tuned as
+        one mix) uses on this graph; returns the report and the settings kept."""
         r = TuneReport()
-        _check(lib().pm_tune(self._h, APPS[app], C.byref(r)))
+        if isinstance(app, str):
+            _check(lib().pm_tune(self._h, APPS[app], C.byref(r)))
+        else:
+            a = np.array([APPS[x] for x in app], np.int32)
+            _check(lib().pm_tune_mix(self._h, a.ctypes.data_as(C.c_void_p), len(a), C.byref(r)))
         return {"trials": r.trials, "default_ms": r.default_ms, "best_ms": r.best_ms,
                 "tunables": self.tunables()}
 

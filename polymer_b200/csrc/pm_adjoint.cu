@@ -124,11 +124,11 @@ int run_weighted_pagerank(pm_graph *g, double damping, double tol, int max_iters
   float *a = (float *)g->scratch_buf(0, (size_t)n * 4);
   float *b = (float *)g->scratch_buf(1, (size_t)n * 4);
   PM_LAUNCH(k_fill_f32, E.grid_for(n, 256, 8), 256, 0, E.stream, a, n, (float)(1.0 / (double)n));
-  const float *w_in = g->w_f32_in.as<float>();
+  const WPair *w_in = ensure_f32_pairs(g);
   const float base = (float)((1.0 - damping) / (double)n);
   const int it = iterate_to_tol(E, a, b, tol, max_iters, resid, "weighted_pagerank",
                                 [&](float *cur, float *nxt) {
-                                  launch_pull_reduce<float>(E, WPR_F{cur, nxt, (float)damping, base},
+                                  launch_pull_reduce<WPair>(E, WPR_F{cur, nxt, (float)damping, base},
                                                             w_in, nullptr, E.d_cnt);
                                 });
   PM_CUDA(cudaMemcpyAsync(d_p, a, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
@@ -143,12 +143,12 @@ int run_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters,
   float *a = (float *)g->scratch_buf(0, (size_t)n * 4);
   float *b = (float *)g->scratch_buf(1, (size_t)n * 4);
   PM_CUDA(cudaMemcpyAsync(a, d_g, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
-  const float *w_out = g->w_f32_out.as<float>();
+  const WPair *w_out = ensure_f32_pairs(g, true);
   int it = 0;
   {
     CsrPull view(E);
     it = iterate_to_tol(E, a, b, tol, max_iters, resid, "pagerank_adjoint", [&](float *cur, float *nxt) {
-      launch_pull_reduce<float>(E, ADJ_F{cur, nxt, d_g, (float)damping}, w_out, nullptr, E.d_cnt);
+      launch_pull_reduce<WPair>(E, ADJ_F{cur, nxt, d_g, (float)damping}, w_out, nullptr, E.d_cnt);
     });
   }
   E.prof.begin("pagerank_adjoint_dw", E.stream);
@@ -164,11 +164,12 @@ void run_spmv_backward(pm_graph *g, const float *d_x, const float *d_gy, float *
   Engine &E = g->E;
   const int64_t m = g->m;
   ensure_out_src(g);
+  const WPair *w_out = d_dx ? ensure_f32_pairs(g, true) : nullptr;
   PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
   E.prof.begin("spmv_backward", E.stream);
   if (d_dx) {
     CsrPull view(E);
-    launch_pull_reduce<float>(E, SPMVB_F{d_gy, d_dx}, g->w_f32_out.as<float>(), nullptr, E.d_cnt);
+    launch_pull_reduce<WPair>(E, SPMVB_F{d_gy, d_dx}, w_out, nullptr, E.d_cnt);
   }
   if (d_dw && m)
     PM_LAUNCH(k_edge_product, E.grid_for(m, 256, 8), 256, 0, E.stream, E.g.out.idx,

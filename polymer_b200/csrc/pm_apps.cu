@@ -291,13 +291,13 @@ void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm) {
   T *x = (T *)g->scratch_buf(0, (size_t)n * sizeof(T));
   T *y = (T *)g->scratch_buf(1, (size_t)n * sizeof(T));
   PM_CUDA(cudaMemcpyAsync(x, d_x0, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
-  const float *w_in = g->w_f32_in.as<float>();
+  const WPair *w_in = ensure_f32_pairs(g);
   E.run_loop(loop_key("spmv", (int)sizeof(T), iters, x, y, w_in, d_norm), [&] {
     T *a = x, *b = y;
     for (int it = 0; it < iters; ++it) {
       PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
       E.prof.begin("spmv", E.stream);
-      launch_pull_reduce<float>(E, SPMV_F<T>{a, b}, w_in, nullptr, E.d_cnt);
+      launch_pull_reduce<WPair>(E, SPMV_F<T>{a, b}, w_in, nullptr, E.d_cnt);
       E.prof.end(E.stream);
       if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
       std::swap(a, b);

@@ -43,7 +43,7 @@ void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
 void set_tunable(pm_graph *g, int key, int64_t value);
 Tunables default_tunables();
 int64_t get_tunable(pm_graph *g, int key);
-void tune(pm_graph *g, int app, pm_tune_report *rep);
+void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep);
 }  // namespace pm
 
 using namespace pm;
@@ -692,7 +692,16 @@ pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
 pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
   return guard([&] {
     enter(g);
-    tune(g, app, report);
+    tune(g, &app, 1, report);
+    finish(g);
+  });
+}
+
+pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report) {
+  return guard([&] {
+    enter(g);
+    need(apps != nullptr, "null apps");
+    tune(g, apps, count, report);
     finish(g);
   });
 }

@@ -343,6 +343,8 @@ void permute_weights_i32(pm_graph *g) {
 }
 void permute_weights_f32(pm_graph *g) {
   const int64_t m = g->m;
+  g->w_f32_pair_in.reset();  // rebuilt from the new weights on first use
+  g->w_f32_pair_out.reset();
   g->w_f32_in.alloc((size_t)std::max<int64_t>(m, 1) * 4);
   if (m)
     PM_LAUNCH(k_gather<float>, grid1d(m), 256, 0, g->E.stream, g->w_f32_out.as<float>(),
@@ -560,6 +562,24 @@ void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float) {
                      seed, wmax, g->w_i32_out.as<int32_t>());
     permute_weights_i32(g);
   }
+}
+
+__global__ void k_make_pairs(const int32_t *__restrict__ idx, const float *__restrict__ w, int64_t m,
+                             WPair *__restrict__ out) {
+  GRID_STRIDE(e, m) out[e] = WPair{idx[e], w[e]};
+}
+
+const WPair *ensure_f32_pairs(pm_graph *g, bool csr) {
+  DevBuf &pairs = csr ? g->w_f32_pair_out : g->w_f32_pair_in;
+  const DevBuf &w = csr ? g->w_f32_out : g->w_f32_in;
+  if (!pairs.p) {
+    if (!w.p) fail(PM_ERR_INVALID_ARG, "graph has no float weights");
+    pairs.alloc((size_t)std::max<int64_t>(g->m, 1) * sizeof(WPair));
+    if (g->m)
+      PM_LAUNCH(k_make_pairs, grid1d(g->m), 256, 0, g->E.stream, csr ? g->E.g.out.idx : g->E.g.in.idx,
+                w.as<float>(), g->m, pairs.as<WPair>());
+  }
+  return pairs.as<WPair>();
 }
 
 void ensure_out_src(pm_graph *g) {

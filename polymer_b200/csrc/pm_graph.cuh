@@ -72,6 +72,8 @@ struct pm_graph {
   pm::DevBuf in_eid;      // CSC slot -> CSR edge id (directed graphs)
   pm::DevBuf out_src;     // source of every CSR edge (built on first use)
   pm::DevBuf w_i32_out, w_i32_in, w_f32_out, w_f32_in;
+  pm::DevBuf w_f32_pair_in;   // {CSC source, float weight} per CSC slot, built on first use
+  pm::DevBuf w_f32_pair_out;  // {CSR destination, float weight} per CSR slot, likewise
   pm::Engine E;
   pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials;
   pm::Counters *h_cnt = nullptr;  // pinned
@@ -108,4 +110,7 @@ void apply_tunables(pm_graph *g, int32_t old_heavy_deg);
 // Writes in_w = out_w[in_eid] (or aliases for symmetric graphs).
 void permute_weights_i32(pm_graph *g);
 void permute_weights_f32(pm_graph *g);
+// The float weights paired with their CSC source ids, or with their CSR
+// destination ids when csr (built once per weights).
+const WPair *ensure_f32_pairs(pm_graph *g, bool csr = false);
 }  // namespace pm

@@ -26,7 +26,7 @@ void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t coun
 namespace {
 
 // Scratch slots of the tuner (the algorithms use 0..5, the boundary 8..12).
-enum { kSlotTuneIn = 14, kSlotTuneOut0 = 15, kSlotTuneOut1 = 16 };
+enum { kSlotTune0 = 14 };  // 14..22
 
 int32_t &field(Tunables &t, int key) {
   switch (key) {
@@ -114,66 +114,83 @@ int64_t get_tunable(pm_graph *g, int key) {
   return field(g->E.tune, key);
 }
 
-void tune(pm_graph *g, int app, pm_tune_report *rep) {
-  Engine &E = g->E;
+// Adds application `app` to the tuned mix: its timed call (with inputs of
+// its own in tuner scratch slots) and the tunables it reads.
+static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &runs, std::vector<int> &keys) {
   const int64_t n = g->n;
-  std::vector<int> keys;
-  std::function<void()> run;
-  std::vector<int32_t> srcs;
-  const float psi[4] = {0.9f, 0.1f, 0.1f, 0.9f};
+  auto slot = [&](int i, size_t bytes) { return g->scratch_buf(kSlotTune0 + i, bytes); };
+  auto add_keys = [&](std::initializer_list<int> ks) {
+    for (int k : ks)
+      if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+  };
   switch (app) {
     case PM_APP_PAGERANK: {
-      float *out = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
-      run = [=] { run_pagerank<float>(g, 3, 0.85, out, nullptr); };
-      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      float *out = (float *)slot(0, (size_t)n * 4);
+      runs.push_back([=] { run_pagerank<float>(g, 3, 0.85, out, nullptr); });
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_SPMV: {
       if (!g->w_f32_out.p) fail(PM_ERR_INVALID_ARG, "graph has no float weights");
-      float *x = (float *)g->scratch_buf(kSlotTuneIn, (size_t)n * 4);
-      float *y = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
+      float *x = (float *)slot(1, (size_t)n * 4);
+      float *y = (float *)slot(2, (size_t)n * 4);
       fill_uniform(g, 0x7E57ull, 0, x, n);
-      run = [=] { run_spmv(g, x, 3, y, nullptr); };
-      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      runs.push_back([=] { run_spmv(g, x, 3, y, nullptr); });
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BP: {
-      float *prior = (float *)g->scratch_buf(kSlotTuneIn, (size_t)n * 8);
-      float *out = (float *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 8);
+      float *prior = (float *)slot(3, (size_t)n * 8);
+      float *out = (float *)slot(4, (size_t)n * 8);
       fill_uniform(g, 0x7E58ull, 1, prior, 2 * n);
-      run = [=] { run_bp(g, prior, psi, 3, out); };
-      keys = {PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM};
+      runs.push_back([=] {
+        const float psi[4] = {0.9f, 0.1f, 0.1f, 0.9f};
+        run_bp(g, prior, psi, 3, out);
+      });
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BFS: {
-      srcs = tune_sources(g, 4);
-      int32_t *p = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
-      int32_t *d = (int32_t *)g->scratch_buf(kSlotTuneOut1, (size_t)n * 4);
-      run = [=] {
+      const std::vector<int32_t> srcs = tune_sources(g, 4);
+      int32_t *p = (int32_t *)slot(5, (size_t)n * 4);
+      int32_t *d = (int32_t *)slot(6, (size_t)n * 4);
+      runs.push_back([=] {
         for (int32_t s : srcs) run_bfs(g, s, p, d, g->m / g->E.tune.bfs_div, nullptr);
-      };
-      keys = {PM_TUNE_BFS_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG};
+      });
+      add_keys({PM_TUNE_BFS_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG});
       break;
     }
     case PM_APP_CC: {
-      int32_t *l = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
-      run = [=] { run_cc(g, l, g->m / g->E.tune.cc_div, nullptr); };
-      keys = {PM_TUNE_CC_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
-              PM_TUNE_PULL_CTAS_PER_SM};
+      int32_t *l = (int32_t *)slot(7, (size_t)n * 4);
+      runs.push_back([=] { run_cc(g, l, g->m / g->E.tune.cc_div, nullptr); });
+      add_keys({PM_TUNE_CC_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
+                PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BF: {
       if (!g->w_i32_out.p) fail(PM_ERR_INVALID_ARG, "graph has no int32 weights");
-      srcs = tune_sources(g, 1);
-      int32_t *d = (int32_t *)g->scratch_buf(kSlotTuneOut0, (size_t)n * 4);
-      run = [=] { run_bellman_ford(g, srcs[0], d, g->m / g->E.tune.bf_div, nullptr); };
-      keys = {PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
-              PM_TUNE_PULL_CTAS_PER_SM};
+      const int32_t src = tune_sources(g, 1)[0];
+      int32_t *d = (int32_t *)slot(8, (size_t)n * 4);
+      runs.push_back([=] { run_bellman_ford(g, src, d, g->m / g->E.tune.bf_div, nullptr); });
+      add_keys({PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
+                PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     default:
       fail(PM_ERR_INVALID_ARG, "unknown application " + std::to_string(app));
   }
+}
+
+void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
+  Engine &E = g->E;
+  if (count < 1 || count > 6) fail(PM_ERR_INVALID_ARG, "application count must be in [1, 6]");
+  std::vector<std::function<void()>> runs;
+  std::vector<int> keys;
+  for (int i = 0; i < count; ++i) add_app(g, apps[i], runs, keys);
+  // the objective: the summed time of the mix
+  std::function<void()> run = [&runs] {
+    for (auto &r : runs) r();
+  };
   int occupancy = 1;  // pull CTAs per SM the device allows for the pull kernel
   {
     int per_sm = 0;
@@ -202,6 +219,9 @@ void tune(pm_graph *g, int app, pm_tune_report *rep) {
   double best_ms = 0.0, default_ms = 0.0;
   try {
     best_ms = default_ms = time_once();
+    // coordinate descent; a second sweep only when the first moved something
+    for (int sweep = 0; sweep < 2; ++sweep) {
+    bool moved = false;
     for (int key : keys) {
       std::vector<int64_t> cands;
       switch (key) {
@@ -228,6 +248,9 @@ void tune(pm_graph *g, int app, pm_tune_report *rep) {
         }
       }
       set_tunable(g, key, keep);
+      moved |= keep != start;
+    }
+    if (!moved) break;
     }
   } catch (...) {
     cudaEventDestroy(a);

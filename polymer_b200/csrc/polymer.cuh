@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pm_common.cuh"
@@ -80,6 +81,36 @@ __device__ __forceinline__ bool set_bit_new(uint32_t *b, int v) {
 template <class W>
 __device__ __forceinline__ W load_w(const W *w, int64_t e) {
   return w ? __ldg(w + e) : W(0);
+}
+
+// Float weights stored beside their source ids, one 8-byte record per CSC
+// slot, so that a pull reads both with one load.
+struct __align__(8) WPair {
+  int32_t src;
+  float w;
+};
+template <class W> struct EdgeT { using type = W; };  // weight type F::edge receives
+template <> struct EdgeT<WPair> { using type = float; };
+
+// Source id of CSC slot e; with paired weights also its weight (into wv).
+template <class W>
+__device__ __forceinline__ int load_src(const int32_t *__restrict__ idx, const W *__restrict__ w, int64_t e,
+                                        typename EdgeT<W>::type &wv) {
+  if constexpr (std::is_same<W, WPair>::value) {
+    const int2 p = __ldg(reinterpret_cast<const int2 *>(w) + e);
+    wv = __int_as_float(p.y);
+    return p.x;
+  } else {
+    return __ldg(idx + e);
+  }
+}
+// Weight of CSC slot e (already loaded by load_src when paired).
+template <class W>
+__device__ __forceinline__ typename EdgeT<W>::type edge_w(const W *w, int64_t e, typename EdgeT<W>::type wv) {
+  if constexpr (std::is_same<W, WPair>::value)
+    return wv;
+  else
+    return load_w(w, e);
 }
 
 // ---------------------------------------------------------------------------
@@ -441,15 +472,16 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f
     static_assert(kChunkEdges % kChunkThreads == 0, "chunk must be a multiple of the CTA");
     constexpr int U = kChunkEdges / kChunkThreads;
     int src[U];
+    typename EdgeT<W>::type wv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t e = e0 + threadIdx.x + (int64_t)u * kChunkThreads;
-      src[u] = e < e1 ? __ldg(g.in.idx + e) : 0;
+      src[u] = e < e1 ? load_src(g.in.idx, w, e, wv[u]) : 0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t e = e0 + threadIdx.x + (int64_t)u * kChunkThreads;
-      if (e < e1) acc = f.combine(acc, f.edge(src[u], r, load_w(w, e)));
+      if (e < e1) acc = f.combine(acc, f.edge(src[u], r, edge_w(w, e, wv[u])));
     }
   }
 #pragma unroll
@@ -527,12 +559,14 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
         const int e0 = off_s[j0] + (c - pos_s[j0]);
         const int cnt = min(WIN, total - c);
         Acc s = f.identity();
+        typename EdgeT<W>::type wv[K];
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          src[k] = (32 * k + lane < cnt) ? __ldg(g.in.idx + e0 + 32 * k + lane) : 0;
+          src[k] = (32 * k + lane < cnt) ? load_src(g.in.idx, w, (int64_t)e0 + 32 * k + lane, wv[k]) : 0;
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (32 * k + lane < cnt) s = f.combine(s, f.edge(src[k], rb + j0, load_w(w, (int64_t)e0 + 32 * k + lane)));
+          if (32 * k + lane < cnt)
+            s = f.combine(s, f.edge(src[k], rb + j0, edge_w(w, (int64_t)e0 + 32 * k + lane, wv[k])));
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) s = f.combine(s, shfl_down(s, d));
         if (lane == 0) acc_s[j0] = f.combine(acc_s[j0], s);
@@ -556,12 +590,13 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
           es[k] = off_s[j] + (q - pos_s[j]);
         }
       }
+      typename EdgeT<W>::type wv[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? __ldg(g.in.idx + es[k]) : 0;
+      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? load_src(g.in.idx, w, es[k], wv[k]) : 0;
       Acc vals[K];
 #pragma unroll
       for (int k = 0; k < K; ++k)
-        vals[k] = (q0 + k < total) ? f.edge(src[k], rb + rows[k], load_w(w, es[k])) : f.identity();
+        vals[k] = (q0 + k < total) ? f.edge(src[k], rb + rows[k], edge_w(w, es[k], wv[k])) : f.identity();
       // Local fold: the first segment is the head, rows that start and end
       // inside the lane are stored directly, the last segment is the tail.
       Acc head = f.identity(), run = f.identity();
