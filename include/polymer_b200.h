@@ -190,6 +190,25 @@ PM_API pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int 
 PM_API pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *ranks,
                       uint32_t mem, double *resid);
 
+/* PageRankDelta.  Replaces PageRankDelta(GA, maxIter)
+ * (numa-PageRankDelta.C:402) with PR_F / PR_Vertex_F_FirstRound /
+ * PR_Vertex_F / PR_Vertex_Reset (64-132) and the loop at 198-230: p = 0,
+ * Delta = 1/n, frontier = all; each round the frontier pushes
+ * Delta[s]/outdeg(s) into nghSum, then every vertex updates (first round:
+ * Delta = damping*(p + nghSum) + (1-damping)/n - p, p += Delta,
+ * Delta -= 1/n; later: Delta = damping*nghSum, p += Delta) and stays in the
+ * frontier when |Delta| > epsilon * p.  The reference uses damping 0.85,
+ * epsilon 0.01 (epsilon2, 407) and runs exactly maxIter rounds (iters >= 1
+ * here: its default of -1 never stops).  threshold: the direction switch of
+ * the rounds after the first (which always pulls); 0 pulls every round as the
+ * reference's threshold 0 does (211); < 0 selects m/20, letting rounds with a
+ * small frontier push with atomics (FP sums then vary in the last bits run
+ * to run).  dtype PM_F32 or PM_F64; ranks: n values.  stats->reached = size
+ * of the final frontier.  The graph must have no self loops. */
+PM_API pm_status pm_pagerank_delta(pm_graph *g, int iters, double damping, double epsilon, int dtype,
+                                   void *ranks, uint32_t mem, int64_t threshold,
+                                   pm_traversal_stats *stats);
+
 /* PageRank (the semantics of pm_pagerank, FP32) on every part of a disjoint
  * union independently, each with its own vertex count, all parts in ONE
  * persistent kernel launch (thread-block clusters take parts from a work

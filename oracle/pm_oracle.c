@@ -270,6 +270,51 @@ PMO_API void pmo_pagerank(int64_t n, const int32_t *off, const int32_t *idx, int
 }
 
 /* ------------------------------------------------------------------------ */
+/* PageRankDelta (numa-PageRankDelta.C): PR_F pushes Delta[s]/outdeg(s) from */
+/* the frontier into nghSum (64-90, DENSE_FORWARD with threshold 0, 211);    */
+/* then a vertexFilter over ALL vertices (215-219): the first round          */
+/* PR_Vertex_F_FirstRound (93-107) sets Delta = d*(p + nghSum) + (1-d)/n - p, */
+/* p += Delta, Delta -= 1/n; later rounds PR_Vertex_F (109-121) set          */
+/* Delta = d*nghSum, p += Delta; a vertex stays in the frontier when          */
+/* |Delta| > eps2 * p; PR_Vertex_Reset zeroes nghSum (124-132).  Starts at    */
+/* p = 0, Delta = 1/n, frontier = all (281-286).  fsize (optional, iters     */
+/* entries): frontier size after each round.                                 */
+/* ------------------------------------------------------------------------ */
+PMO_API void pmo_pagerank_delta(int64_t n, const int32_t *off, const int32_t *idx, int iters,
+                                double damping, double eps2, double *p_out, int64_t *fsize) {
+  double *p = (double *)calloc((size_t)n, sizeof(double));
+  double *delta = (double *)malloc((size_t)n * sizeof(double));
+  double *ngh = (double *)calloc((size_t)n, sizeof(double));
+  unsigned char *F = (unsigned char *)malloc((size_t)n);
+  const double one_over_n = 1.0 / (double)n, added = (1.0 - damping) * one_over_n;
+  for (int64_t i = 0; i < n; ++i) { delta[i] = one_over_n; F[i] = 1; }
+  for (int it = 0; it < iters; ++it) {
+    for (int64_t s = 0; s < n; ++s) {
+      if (!F[s]) continue;
+      const int64_t deg = off[s + 1] - off[s];
+      for (int64_t e = off[s]; e < off[s + 1]; ++e) ngh[idx[e]] += delta[s] / (double)deg;
+    }
+    int64_t cnt = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (it == 0) {
+        delta[i] = damping * (p[i] + ngh[i]) + added - p[i];
+        p[i] += delta[i];
+        delta[i] -= one_over_n;
+      } else {
+        delta[i] = ngh[i] * damping;
+        p[i] += delta[i];
+      }
+      F[i] = fabs(delta[i]) > eps2 * p[i];
+      cnt += F[i];
+      ngh[i] = 0.0;
+    }
+    if (fsize) fsize[it] = cnt;
+  }
+  memcpy(p_out, p, (size_t)n * sizeof(double));
+  free(p); free(delta); free(ngh); free(F);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Personalised PageRank for k seeds (no reference; built from PR_F's push  */
 /* p[s]/outdeg(s), numa-PageRank.C:87-90, and PR_Vertex_F's damping,        */
 /* 125-137, with the teleport going to the seed):                           */

@@ -67,6 +67,8 @@ def lib():
             "pmo_pagerank": (None, [i64, i32p, i32p, C.c_int, C.c_double, f64p, C.c_void_p]),
             "pmo_spmv": (None, [i64, i32p, i32p, f64p, f64p, C.c_int, f64p]),
             "pmo_ppr": (None, [i64, i32p, i32p, i32p, C.c_int, C.c_int, C.c_double, f64p]),
+            "pmo_pagerank_delta": (None, [i64, i32p, i32p, C.c_int, C.c_double, C.c_double, f64p,
+                                          C.c_void_p]),
             "pmo_weighted_pagerank": (C.c_int, [i64, i32p, i32p, f64p, C.c_double, C.c_double,
                                                 C.c_int, f64p]),
             "pmo_pagerank_adjoint": (C.c_int, [i64, i32p, i32p, f64p, C.c_double, C.c_double, C.c_int,
@@ -198,6 +200,16 @@ def pagerank(g: Graph, iters: int, damping: float = 0.85, with_resid: bool = Fal
     resid = np.zeros(max(iters, 1), np.float64)
     lib().pmo_pagerank(g.n, g.off, _idx(g), iters, damping, out, _ptr(resid))
     return (out, resid[:iters]) if with_resid else out
+
+
+def pagerank_delta(g: Graph, iters: int, damping: float = 0.85, eps2: float = 0.01,
+                   with_frontier: bool = False):
+    """PageRankDelta restatement (FP64): p after `iters` rounds (and the
+    frontier size after each round)."""
+    p = np.empty(g.n, np.float64)
+    fs = np.zeros(max(iters, 1), np.int64)
+    lib().pmo_pagerank_delta(g.n, g.off, _idx(g), iters, damping, eps2, p, fs.ctypes.data_as(C.c_void_p))
+    return (p, fs[:iters]) if with_frontier else p
 
 
 def ppr(g: Graph, seeds, iters: int, damping: float = 0.85) -> np.ndarray:
@@ -375,6 +387,18 @@ def ref_pagerank(path: str, iters: int, binary: bool = True, threads=None, resul
     out, t = _run(args, threads, timeout)
     if not result:
         return None, t
+    vals = re.findall(r"^(\d+)\t([0-9.eE+-]+)$", out, re.M)
+    r = np.zeros(len(vals), np.float64)
+    for i, v in vals:
+        r[int(i)] = float(v)
+    return r, t
+
+
+def ref_pagerank_delta(path: str, iters: int, binary: bool = True, threads=None, timeout=600):
+    """numa-PageRankDelta <g> <iters> -result -a [-b]; returns (p, seconds)."""
+    args = [os.path.join(REF_DIR, "numa-PageRankDelta"), path, str(iters), "-result", "-a",
+            "-b" if binary else "-t"]
+    out, t = _run(args, threads, timeout)
     vals = re.findall(r"^(\d+)\t([0-9.eE+-]+)$", out, re.M)
     r = np.zeros(len(vals), np.float64)
     for i, v in vals:

@@ -25,7 +25,7 @@ import numpy as np
 
 __all__ = [
     "Graph", "PolymerError", "PageRank", "BFS", "BFSMulti", "Components", "BellmanFord",
-    "BellmanFordMulti", "SPMV",
+    "BellmanFordMulti", "PageRankDelta", "SPMV",
     "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
 ]
 
@@ -94,6 +94,8 @@ def lib():
         "pm_bfs_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bellman_ford_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_ppr": [vp, vp, C.c_int, C.c_int, C.c_double, vp, u32],
+        "pm_pagerank_delta": [vp, C.c_int, C.c_double, C.c_double, C.c_int, vp, u32, i64,
+                              C.POINTER(TraversalStats)],
         "pm_graph_create_er_batch": [C.c_int, i64, i64, C.c_int, u64, C.c_int, C.POINTER(vp)],
         "pm_graph_set_parts": [vp, vp, C.c_int],
         "pm_graph_get_parts": [vp, vp, C.POINTER(C.c_int)],
@@ -440,6 +442,19 @@ def PageRank(g: Graph, maxIter: int = 20, damping: float = 0.85, dtype=np.float6
                              PM_F64 if dt == np.float64 else PM_F32, pr, mem,
                              res.ctypes.data_as(C.c_void_p) if resid else None))
     return (ranks, res[:maxIter]) if resid else ranks
+
+
+def PageRankDelta(g: Graph, maxIter: int = 10, damping: float = 0.85, epsilon: float = 0.01,
+                  dtype=np.float64, threshold: int = -1, device_out=None, stats: bool = False, out=None):
+    """Delta-propagating PageRank (numa-PageRankDelta.C): only vertices whose
+    rank moved by more than epsilon of itself push their change."""
+    dt = np.float64 if np.dtype(dtype) == np.float64 else np.float32
+    ranks, pr, mem = _out(device_out, g.n, dt, out)
+    st = TraversalStats()
+    _check(lib().pm_pagerank_delta(g.handle, int(maxIter), float(damping), float(epsilon),
+                                   PM_F64 if dt == np.float64 else PM_F32, pr, mem, int(threshold),
+                                   C.byref(st)))
+    return (ranks, st.as_dict()) if stats else ranks
 
 
 def WeightedPageRank(g: Graph, damping: float = 0.85, tol: float = 1e-6, max_iters: int = 1000,

@@ -387,6 +387,136 @@ void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out) {
                           E.stream));
 }
 
+// ===========================================================================
+// PageRankDelta  (numa-PageRankDelta.C:64-132 PR_F / PR_Vertex_F_FirstRound /
+// PR_Vertex_F / PR_Vertex_Reset, loop 198-230)
+// Only vertices whose rank moved by more than eps2 of itself push their
+// change.  c[s] holds Delta[s]/outdeg(s) for s in the frontier and 0 elsewhere.
+// Dense rounds pull sum c[s] over the CSC and commit the vertexFilter of
+// every row (the reference's filter over All) into a second array; sparse
+// rounds push c[s] to the out-neighbours with atomicAdd into ngh, then clear
+// c on the old frontier and commit the touched vertices only (an untouched
+// vertex gets Delta = 0: its rank stays and it leaves the frontier).  The
+// first round (p = 0, Delta = 1/n, frontier = all) always runs dense.
+// ===========================================================================
+template <class T>
+__device__ __forceinline__ bool prd_commit(T acc, bool first, T damping, T added, T one_over_n, T eps2,
+                                           T &p, T &c, int deg) {
+  T dl;
+  if (first) {
+    const T p0 = p;
+    dl = damping * (p0 + acc) + added - p0;
+    p = p0 + dl;
+    dl -= one_over_n;
+  } else {
+    dl = acc * damping;
+    p += dl;
+  }
+  const bool in = fabs(dl) > eps2 * p;
+  c = in && deg > 0 ? dl / T(deg) : T(0);
+  return in;
+}
+
+template <class T>
+struct PRD_F {
+  const T *c_cur;
+  T *c_next;
+  T *p;
+  T *ngh;  // sparse rounds: atomically summed pushes
+  const int32_t *out_off;
+  T damping, added, one_over_n, eps2;
+  bool first;
+  using Acc = T;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int) const {
+    atomicAdd(ngh + d, __ldg(c_cur + s));
+    return true;
+  }
+  __device__ __forceinline__ Acc identity() const { return T(0); }
+  __device__ __forceinline__ Acc edge(int s, int, int) const { return __ldg(c_cur + s); }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
+    T pd = p[d], cd;
+    const bool in = prd_commit(acc, first, damping, added, one_over_n, eps2, pd, cd,
+                               __ldg(out_off + d + 1) - __ldg(out_off + d));
+    p[d] = pd;
+    c_next[d] = cd;
+    return in;
+  }
+};
+
+template <class T>
+struct PRD_Clear {
+  T *c;
+  __device__ __forceinline__ void operator()(int v) const { c[v] = T(0); }
+};
+
+template <class T>
+struct PRD_SparseCommit {
+  T *c, *p, *ngh;
+  const int32_t *out_off;
+  T damping, eps2;
+  __device__ __forceinline__ bool operator()(int v) const {
+    const T acc = ngh[v];
+    ngh[v] = T(0);
+    T pv = p[v], cv;
+    const bool in = prd_commit(acc, false, damping, T(0), T(0), eps2, pv, cv,
+                               __ldg(out_off + v + 1) - __ldg(out_off + v));
+    p[v] = pv;
+    c[v] = cv;
+    return in;
+  }
+};
+
+template <class T>
+__global__ void k_prd_init(T *c, T *p, T *ngh, const int32_t *out_off, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const T d0 = T(1) / T(n);
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const int deg = out_off[v + 1] - out_off[v];
+    c[v] = deg > 0 ? d0 / T(deg) : T(0);
+    p[v] = T(0);
+    ngh[v] = T(0);
+  }
+}
+
+template <class T>
+void run_pagerank_delta(pm_graph *g, int iters, double damping, double eps2, T *d_out, int64_t threshold,
+                        pm_traversal_stats *st) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  T *c0 = (T *)g->scratch_buf(0, (size_t)n * sizeof(T));
+  T *c1 = (T *)g->scratch_buf(1, (size_t)n * sizeof(T));
+  T *p = (T *)g->scratch_buf(2, (size_t)n * sizeof(T));
+  T *ngh = (T *)g->scratch_buf(3, (size_t)n * sizeof(T));
+  PM_LAUNCH((k_prd_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, c0, p, ngh, E.g.out.off, n);
+  VertexSubset cur = g->subset(0), next = g->subset(1);
+  subset_all(E, cur);
+  const T one_over_n = T(1.0 / (double)n), added = T((1.0 - damping) / (double)n);
+  pm_traversal_stats s{};
+  E.tag = "pagerank_delta";
+  for (int it = 0; it < iters; ++it) {
+    const bool first = it == 0;
+    PRD_F<T> f{c0, c1, p, ngh, E.g.out.off, (T)damping, added, one_over_n, (T)eps2, first};
+    bool dense = false;
+    s.edges_visited += cur.edges;
+    // the first round commits every vertex, so it always pulls
+    edgeMapReduce<int>(E, cur, f, next, first ? 0 : threshold, nullptr, nullptr, &dense);
+    if (dense) {
+      std::swap(c0, c1);
+      std::swap(cur, next);
+    } else {
+      vertexMap(E, cur, PRD_Clear<T>{c0});
+      vertexFilter(E, next, PRD_SparseCommit<T>{c0, p, ngh, E.g.out.off, (T)damping, (T)eps2}, cur);
+    }
+    s.rounds++;
+    s.dense_rounds += dense;
+  }
+  s.reached = cur.size;
+  PM_CUDA(cudaMemcpyAsync(d_out, p, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, E.stream));
+  if (st) *st = s;
+}
+
 // explicit instantiations used by the C ABI
 template void run_pagerank<float>(pm_graph *, int, double, float *, double *);
 template void run_pagerank<double>(pm_graph *, int, double, double *, double *);
@@ -394,5 +524,8 @@ template void run_spmv<float>(pm_graph *, const float *, int, float *, double *)
 template void run_spmv<double>(pm_graph *, const double *, int, double *, double *);
 template void run_bp<float>(pm_graph *, const float *, const float *, int, float *);
 template void run_bp<double>(pm_graph *, const double *, const double *, int, double *);
+template void run_pagerank_delta<float>(pm_graph *, int, double, double, float *, int64_t, pm_traversal_stats *);
+template void run_pagerank_delta<double>(pm_graph *, int, double, double, double *, int64_t,
+                                         pm_traversal_stats *);
 
 }  // namespace pm

@@ -21,6 +21,9 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
 template <class T>
 void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_resid);
 template <class T>
+void run_pagerank_delta(pm_graph *g, int iters, double damping, double eps2, T *d_out, int64_t threshold,
+                        pm_traversal_stats *st);
+template <class T>
 void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm);
 template <class T>
 void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out);
@@ -441,6 +444,30 @@ pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *r
       run_pagerank<float>(g, iters, damping, (float *)dr, dres);
     if (mem == PM_MEM_HOST) from_device(g, ranks, dr, bytes, mem);
     if (resid && iters > 0) from_device(g, resid, dres, (size_t)iters * 8, PM_MEM_HOST);
+    finish(g);
+  });
+}
+
+pm_status pm_pagerank_delta(pm_graph *g, int iters, double damping, double epsilon, int dtype, void *ranks,
+                            uint32_t mem, int64_t threshold, pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(ranks != nullptr, "null ranks");
+    need(iters >= 1, "iters must be >= 1 (the reference loops until maxIter)");
+    need(damping > 0.0 && damping < 1.0, "damping must be in (0, 1)");
+    need(epsilon >= 0.0 && std::isfinite(epsilon), "epsilon must be finite and >= 0");
+    need(dtype == PM_F32 || dtype == PM_F64, "dtype must be PM_F32 or PM_F64");
+    need(!g->has_self_loops,
+         "PageRankDelta needs a graph without self loops (create it with PM_GRAPH_SKIP_SELF_LOOPS)");
+    const size_t bytes = (size_t)g->n * (dtype == PM_F64 ? 8 : 4);
+    void *dr = mem == PM_MEM_DEVICE ? ranks : g->scratch_buf(kSlotOut0, bytes);
+    const int64_t thr = threshold < 0 ? g->m / 20 : threshold;
+    if (dtype == PM_F64)
+      run_pagerank_delta<double>(g, iters, damping, epsilon, (double *)dr, thr, stats);
+    else
+      run_pagerank_delta<float>(g, iters, damping, epsilon, (float *)dr, thr, stats);
+    if (mem == PM_MEM_HOST) from_device(g, ranks, dr, bytes, mem);
     finish(g);
   });
 }

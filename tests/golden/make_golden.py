@@ -56,6 +56,13 @@ def main():
                         pagerank10=pr, spmv_w=w, spmv5=sp)
     out["rmat10_directed"] = (g.n, g.m)
 
+    # --- directed scale-10 R-MAT: PageRankDelta, 3 and 10 rounds ----------
+    prd3, _ = O.ref_pagerank_delta(base, 3, threads=4)
+    prd10, _ = O.ref_pagerank_delta(base, 10, threads=4)
+    np.savez_compressed(os.path.join(HERE, "rmat10_prdelta.npz"), off=g.off, idx=g.idx,
+                        prdelta3=prd3, prdelta10=prd10)
+    out["rmat10_prdelta"] = (g.n, g.m)
+
     # --- symmetric scale-10 R-MAT: CC, BFS parents -------------------------
     gs = O.rmat_graph(10, 16, symmetric=True)
     bs = os.path.join(d, "rmat10s")

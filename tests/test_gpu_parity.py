@@ -329,6 +329,45 @@ def test_spmv_f64_matches_oracle_and_reference(pm, oracle):
 
 
 # --------------------------------------------------------------------------
+RL1_PRD_F32 = 1e-5   # FP32 PageRankDelta (measured 1.1e-7 at scale 16; a vertex within FP32
+                     # rounding of |Delta| = eps2 * p could take the other side of the test)
+
+
+@pytest.mark.parametrize("threshold", [0, -1, 1 << 40])
+def test_pagerank_delta_f64_matches_oracle(pm, oracle, threshold):
+    og = oracle.rmat_graph(14, 16)
+    ref, fs = oracle.pagerank_delta(og, 10, with_frontier=True)
+    with dev_graph(pm, og) as g:
+        p, st = pm.PageRankDelta(g, 10, dtype=np.float64, threshold=threshold, stats=True)
+    assert np.allclose(p, ref, rtol=1e-9, atol=1e-15)
+    assert st["rounds"] == 10 and st["reached"] == fs[-1]
+    if threshold == 0:
+        assert st["dense_rounds"] == 10   # the reference's threshold 0: every round pulls
+    if threshold == 1 << 40:
+        assert st["dense_rounds"] == 1    # only the first round, which commits every vertex
+
+
+def test_pagerank_delta_reference_fixture(pm):
+    z = load("rmat10_prdelta.npz")
+    with pm.Graph.from_csr(z["off"], z["idx"]) as g:
+        for iters, key in ((3, "prdelta3"), (10, "prdelta10")):
+            p = pm.PageRankDelta(g, iters, dtype=np.float64, threshold=0)
+            assert np.allclose(p, z[key], rtol=2e-9, atol=0), key
+
+
+def test_pagerank_delta_f32_rel_l1(pm, oracle):
+    og = oracle.rmat_graph(16, 16)
+    ref = oracle.pagerank_delta(og, 10)
+    with dev_graph(pm, og) as g:
+        for thr in (0, -1):
+            p = pm.PageRankDelta(g, 10, dtype=np.float32, threshold=thr)
+            err = rel_l1(p, ref)
+            print("PageRankDelta FP32 threshold %d rel-L1 %.3g" % (thr, err))
+            assert err < RL1_PRD_F32, err
+        with pytest.raises(pm.PolymerError):
+            pm.PageRankDelta(g, 0)
+
+
 @pytest.mark.parametrize("k", [32, 3])
 def test_ppr_matches_oracle(pm, oracle, k):
     og = oracle.rmat_graph(14, 16)

@@ -132,6 +132,15 @@ def test_ppr_restatement(oracle):
         assert x[s, j] >= 0.15
 
 
+def test_pagerank_delta_matches_reference_fixture(oracle):
+    z = np.load(os.path.join(GOLDEN, "rmat10_prdelta.npz"))
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    for iters, key in ((3, "prdelta3"), (10, "prdelta10")):
+        p, fs = oracle.pagerank_delta(g, iters, with_frontier=True)
+        assert np.allclose(p, z[key], rtol=2e-9, atol=0), key  # the reference prints %.9e
+    assert fs[0] > fs[-1] and fs[-1] == 0  # the frontier drains within 10 rounds here
+
+
 def test_depths_from_parents_rejects_cycles(oracle):
     with pytest.raises(ValueError):
         oracle.bfs_depths_from_parents(np.array([0, 2, 1], np.int32), 0)
@@ -145,6 +154,8 @@ def test_live_reference_scale12(oracle, tmp_path):
     base = oracle.write_binary(g, str(tmp_path / "g"))
     ref, _ = oracle.ref_pagerank(base, 10, threads=4)
     assert np.allclose(oracle.pagerank(g, 10), ref, rtol=2e-9, atol=0)
+    prd, _ = oracle.ref_pagerank_delta(base, 8, threads=4)
+    assert np.allclose(oracle.pagerank_delta(g, 8), prd, rtol=2e-9, atol=0)
     gs = oracle.rmat_graph(12, 16, symmetric=True)
     bs = oracle.write_binary(gs, str(tmp_path / "s"))
     lab, _ = oracle.ref_components(bs, threads=4)
