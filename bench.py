@@ -408,6 +408,49 @@ def batched_block(pm, suite, reps=3):
     return res
 
 
+def ingest_block(pm, reps=3):
+    """PBBS text ingest (pm_graph_load_pbbs): directed R-MAT scale 20 written
+    as an AdjacencyGraph text file, read back with the header on the host and
+    the body tokenised and parsed on the GPU, then validated and transposed
+    (CSC) on the device; host clock around the synchronous call, file in the
+    page cache after the first read.  Also the binary triple."""
+    import tempfile
+    with pm.Graph.rmat(20, 16, seed=SEED_GRAPH) as G:
+        off, idx = G.csr()
+    d = tempfile.mkdtemp(prefix="pm_ingest_")
+    path = os.path.join(d, "rmat20.adj")
+    with open(path, "w") as f:
+        f.write("AdjacencyGraph\n%d\n%d\n" % (len(off) - 1, len(idx)))
+    with open(path, "a") as f:
+        off[:-1].tofile(f, sep="\n")
+        f.write("\n")
+        idx.tofile(f, sep="\n")
+        f.write("\n")
+    base = os.path.join(d, "rmat20b")
+    with open(base + ".config", "w") as f:
+        f.write("%d\n" % (len(off) - 1))
+    idx.astype(np.int32).tofile(base + ".adj")
+    off[:-1].astype(np.int32).tofile(base + ".idx")
+    size = os.path.getsize(path)
+    out = {"graph": "directed R-MAT scale 20 (n=%d, m=%d)" % (len(off) - 1, len(idx)), "text_bytes": size}
+    for name, kw, p in (("text", {}, path), ("binary", {"binary": True}, base)):
+        times = []
+        for _ in range(reps + 1):
+            t0 = time.perf_counter()
+            with pm.Graph.load_pbbs(p, **kw) as g:
+                assert g.m == len(idx)
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times[1:])
+        out[name] = {"seconds": round(t, 4), "medges_per_s": round(len(idx) / t / 1e6, 1)}
+        if name == "text":
+            out[name]["mb_per_s"] = round(size / t / 1e6, 1)
+    for fn in (path, base + ".config", base + ".adj", base + ".idx"):
+        os.remove(fn)
+    os.rmdir(d)
+    out["timing"] = "host clock around the call (file read, parse, validation, CSC build), median of %d" % reps
+    return out
+
+
 def adjoint_block(pm, torch, dev, reps=3):
     """Weighted PageRank on directed R-MAT scale 20 with
     lognormal(0,1) weights normalised per source row, damping 0.85, solved to
@@ -713,6 +756,7 @@ def main():
     if not args.no_batched:
         line["batched"] = batched_block(pm, suite)
         line["adjoint"] = adjoint_block(pm, torch, suite.dev)
+        line["ingest"] = ingest_block(pm)
     if not args.no_e2e:
         line["e2e"] = e2e_run(pm, suite, args.e2e_steps)
     if dist:

@@ -69,6 +69,22 @@ typedef struct pm_graph pm_graph;
 PM_API pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t n, int64_t m,
                           uint32_t flags, uint32_t mem, int device, pm_graph **out);
 
+/* Read a PBBS graph file into a device graph.  Replaces readGraph() /
+ * readGraphSkipRing() / readWghGraph() (IO-numa.h:112-160, 318-470, 739-755).
+ * Text (default): "AdjacencyGraph" or "WeightedAdjacencyGraph", then n, m,
+ * the n offsets, the m edge ids and, when weighted, m int32 weights, all
+ * separated by whitespace; the header is read on the host, the body is
+ * tokenised and parsed on the GPU.  With PM_LOAD_BINARY, path is the base of
+ * <path>.config (n as text), <path>.adj (m uint32 ids) and <path>.idx (n int32
+ * offsets).  Other flags as pm_graph_create (PM_GRAPH_SYMMETRIC,
+ * PM_GRAPH_SKIP_SELF_LOOPS: weights of dropped self loops go with them).
+ * Weighted files set the int32 weights (as pm_graph_set_weights_i32).
+ * PM_ERR_BAD_GRAPH for a bad header, a count that does not match, a word
+ * that is not an integer or a value outside int32; PM_ERR_INVALID_ARG when a
+ * file cannot be opened. */
+#define PM_LOAD_BINARY 16u
+PM_API pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out);
+
 /* Build the seeded synthetic R-MAT graph (a,b,c,d = .57,.19,.19,.05;
  * n = 2^scale, n*edge_factor draws, self loops and duplicates removed,
  * sorted by source) directly on the device.  The same generator, evaluated

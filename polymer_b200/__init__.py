@@ -32,7 +32,7 @@ __all__ = [
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_b200.so")
 
 PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
-PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS = 2, 4
+PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY = 2, 4, 16
 PM_F32, PM_F64 = 0, 1
 BF_INF = 1073741823
 
@@ -121,6 +121,7 @@ def lib():
         "pm_host_alloc": [u64, C.POINTER(vp)],
         "pm_host_free": [vp],
         "pm_graph_set_tunable": [vp, C.c_int, i64],
+        "pm_graph_load_pbbs": [C.c_char_p, u32, C.c_int, C.POINTER(vp)],
         "pm_graph_get_tunable": [vp, C.c_int, C.POINTER(i64)],
         "pm_tune": [vp, C.c_int, C.POINTER(TuneReport)],
         "pm_tune_mix": [vp, vp, C.c_int, C.POINTER(TuneReport)],
@@ -200,6 +201,17 @@ class Graph:
         """PBBS AdjacencyGraph arrays: n offsets (no trailing m) and m edges."""
         off = np.append(np.ascontiguousarray(offsets_n, np.int32), np.int32(len(edges)))
         return cls.from_csr(off, np.ascontiguousarray(edges, np.int32), **kw)
+
+    @classmethod
+    def load_pbbs(cls, path: str, symmetric: bool = False, skip_self_loops: bool = False,
+                  binary: bool = False, device: int = 0) -> "Graph":
+        """Read a PBBS file (text, parsed on the GPU; or the binary
+        .config/.adj/.idx triple under base name `path`)."""
+        h = C.c_void_p()
+        flags = (PM_GRAPH_SYMMETRIC if symmetric else 0) | (PM_GRAPH_SKIP_SELF_LOOPS if skip_self_loops else 0) \
+            | (PM_LOAD_BINARY if binary else 0)
+        _check(lib().pm_graph_load_pbbs(os.fsencode(path), flags, device, C.byref(h)))
+        return cls(h)
 
     @classmethod
     def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 0x5EED0001, symmetric: bool = False,

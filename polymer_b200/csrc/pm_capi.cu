@@ -9,7 +9,11 @@
 
 namespace pm {
 long long launches(bool reset);
-void ingest_csr(pm_graph *g, bool skip_self_loops);
+void ingest_csr(pm_graph *g, bool skip_self_loops, DevBuf *w = nullptr);
+void parse_pbbs_text(pm_graph *g, const char *path, DevBuf &off, DevBuf &idx, DevBuf &w, int64_t &n,
+                     int64_t &m);
+void read_pbbs_binary(const char *base, std::vector<int32_t> &off, std::vector<int32_t> &idx, int64_t &n,
+                      int64_t &m);
 void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed);
 void gen_weights(pm_graph *g, uint64_t seed, int32_t wmax, bool is_float);
 void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t count);
@@ -154,6 +158,42 @@ pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t 
       to_device(g, g->out.idx.p, edges, (size_t)m * 4, mem);
       ingest_csr(g, (flags & PM_GRAPH_SKIP_SELF_LOOPS) != 0);
       finish_graph(g);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(path != nullptr, "null path");
+    pm_graph *g = new_graph(device, (flags & PM_GRAPH_SYMMETRIC) != 0);
+    try {
+      DevBuf w;
+      int64_t n = 0, m = 0;
+      if (flags & PM_LOAD_BINARY) {
+        std::vector<int32_t> off, idx;
+        read_pbbs_binary(path, off, idx, n, m);
+        g->out.off.alloc((size_t)(n + 1) * 4);
+        g->out.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+        to_device(g, g->out.off.p, off.data(), (size_t)(n + 1) * 4, PM_MEM_HOST);
+        to_device(g, g->out.idx.p, idx.data(), (size_t)m * 4, PM_MEM_HOST);
+        finish(g);
+      } else {
+        parse_pbbs_text(g, path, g->out.off, g->out.idx, w, n, m);
+      }
+      g->n = n;
+      g->m = m;
+      ingest_csr(g, (flags & PM_GRAPH_SKIP_SELF_LOOPS) != 0, &w);
+      finish_graph(g);
+      if (w.p) {
+        g->w_i32_out = std::move(w);
+        permute_weights_i32(g);
+      }
     } catch (...) {
       delete g;
       throw;

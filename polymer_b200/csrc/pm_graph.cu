@@ -352,8 +352,9 @@ void permute_weights_f32(pm_graph *g) {
   PM_CUDA(cudaStreamSynchronize(g->E.stream));
 }
 
-// Validate a CSR already on the device; optionally drop self loops.
-void ingest_csr(pm_graph *g, bool skip_self_loops) {
+// Validate a CSR already on the device; optionally drop self loops (and
+// the matching entries of w, int32 weights in CSR order, when given).
+void ingest_csr(pm_graph *g, bool skip_self_loops, DevBuf *w) {
   cudaStream_t st = g->E.stream;
   const int64_t n = g->n, m = g->m;
   DevBuf err(8);
@@ -393,6 +394,13 @@ void ingest_csr(pm_graph *g, bool skip_self_loops) {
             noff.as<int32_t>());
   PM_LAUNCH(k_compact_edges, grid1d(m), 256, 0, st, g->out.idx.as<int32_t>(), keep.as<int32_t>(),
             pre.as<int32_t>(), m, nidx.as<int32_t>());
+  if (w && w->p) {
+    DevBuf nw((size_t)std::max<int32_t>(m_new, 1) * 4);
+    PM_LAUNCH(k_compact_edges, grid1d(m), 256, 0, st, w->as<int32_t>(), keep.as<int32_t>(), pre.as<int32_t>(),
+              m, nw.as<int32_t>());
+    PM_CUDA(cudaStreamSynchronize(st));
+    *w = std::move(nw);
+  }
   PM_CUDA(cudaStreamSynchronize(st));
   g->out.off = std::move(noff);
   g->out.idx = std::move(nidx);
