@@ -116,6 +116,29 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _hash(seed, c):
+    M = (1 << 64) - 1
+    z = (seed + (c + 1) * 0x9E3779B97F4A7C15) & M
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+    return z ^ (z >> 31)
+
+
+def pick_sources(off, k, seed):
+    """k distinct seeded sources with out-edges (rank r of a replica run uses
+    seed SEED_SRC + r, so ranks traverse from different sources)."""
+    n = len(off) - 1
+    out, seen = [], set()
+    j = 0
+    while len(out) < k and j < 64 * n:
+        v = _hash(seed, j) % n
+        j += 1
+        if off[v + 1] > off[v] and v not in seen:
+            seen.add(v)
+            out.append(int(v))
+    return out
+
+
 # ---------------------------------------------------------------------------
 class Suite:
     """The two device-resident graphs and the per-step application calls."""
@@ -157,24 +180,10 @@ class Suite:
         self.tuning = rep
         return rep
 
-    @staticmethod
-    def _hash(seed, c):
-        M = (1 << 64) - 1
-        z = (seed + (c + 1) * 0x9E3779B97F4A7C15) & M
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
-        return z ^ (z >> 31)
+    _hash = staticmethod(_hash)
 
     def _pick_sources(self, off, k, seed):
-        n = len(off) - 1
-        out = []
-        j = 0
-        while len(out) < k and j < 64 * n:
-            v = self._hash(seed, j) % n
-            j += 1
-            if off[v + 1] > off[v] and v not in out:
-                out.append(int(v))
-        return out
+        return pick_sources(off, k, seed)
 
     def _uniform01(self, n, seed):
         return self.pm.uniform_f32(self.B, n, seed, open_interval=False).cpu().numpy()
@@ -648,6 +657,18 @@ def run_reference(args):
     return 0
 
 
+def aggregate_ranks(dist, ms_step, edges, device):
+    """Whole-job numbers of a replica run: the slowest rank's step time (max
+    over ranks) and the edges every rank counted (sum over ranks)."""
+    import torch
+    t = torch.tensor([ms_step, float(edges)], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[1])
+
+
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
@@ -689,14 +710,11 @@ def main():
     clk = clocks.stop()
     pr_ms, pr_passes = suite.B.profile_read("pagerank", reset=True)
     suite.B.profile(False)
+    if dist:
+        dist.barrier()
     ms_step = tot_ms / args.steps
     if dist:
-        t = torch.tensor([ms_step, float(tot_edges)], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_step, tot_edges_all = float(mx[0]), float(sm[1])
+        ms_step, tot_edges_all = aggregate_ranks(dist, ms_step, tot_edges, "cuda")
     else:
         tot_edges_all = float(tot_edges)
     value = tot_edges_all / args.steps / (ms_step / 1e3) / 1e9
