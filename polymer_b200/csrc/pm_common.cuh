@@ -9,19 +9,28 @@
 
 #include "polymer_b200.h"
 
+// C++ symbols the engine templates call from code compiled outside the
+// library (an application's own functors, include/polymer_b200_engine.cuh)
+// are exported; everything else stays hidden.
+#if defined(__GNUC__)
+#define PM_CXX_API __attribute__((visibility("default")))
+#else
+#define PM_CXX_API
+#endif
+
 namespace pm {
 
 // Internal failures travel as exceptions and become a pm_status at the C ABI.
-struct Failure : std::runtime_error {
+struct PM_CXX_API Failure : std::runtime_error {
   pm_status status;
   Failure(pm_status s, const std::string &msg) : std::runtime_error(msg), status(s) {}
 };
 
-[[noreturn]] void fail(pm_status s, const std::string &msg);
-void set_last_error(const std::string &msg);  // text returned by pm_last_error()
-[[noreturn]] void fail_cuda(cudaError_t e, const char *what, const char *file, int line);
-void count_launch(int n = 1);
-long long launches(bool reset);
+[[noreturn]] PM_CXX_API void fail(pm_status s, const std::string &msg);
+PM_CXX_API void set_last_error(const std::string &msg);  // text returned by pm_last_error()
+[[noreturn]] PM_CXX_API void fail_cuda(cudaError_t e, const char *what, const char *file, int line);
+PM_CXX_API void count_launch(int n = 1);
+PM_CXX_API long long launches(bool reset);
 
 #define PM_CUDA(call)                                                        \
   do {                                                                       \

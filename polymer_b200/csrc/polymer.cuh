@@ -1073,14 +1073,14 @@ struct Engine {
 };
 
 // Recount s.size / s.edges from s.bits (vertexCounter, polymer.h:2311-2338).
-void subset_recount(Engine &E, VertexSubset &s);
+PM_CXX_API void subset_recount(Engine &E, VertexSubset &s);
 // Make sure s.queue holds s (compaction of the bitmap).
-void subset_to_queue(Engine &E, VertexSubset &s);
+PM_CXX_API void subset_to_queue(Engine &E, VertexSubset &s);
 // Single vertex frontier.
-void subset_single(Engine &E, VertexSubset &s, int32_t v);
+PM_CXX_API void subset_single(Engine &E, VertexSubset &s, int32_t v);
 // All vertices.
-void subset_all(Engine &E, VertexSubset &s);
-void subset_clear(Engine &E, VertexSubset &s);
+PM_CXX_API void subset_all(Engine &E, VertexSubset &s);
+PM_CXX_API void subset_clear(Engine &E, VertexSubset &s);
 
 // Direction switch of edgeMap (polymer.h:2247, 2260): dense when
 // |F| + outdeg(F) >= threshold.

@@ -78,3 +78,21 @@ def test_default_tunables_host_only():
         for k, v in defaults.items():
             pm.set_default_tunable(k, v)
     assert {k: pm.get_default_tunable(k) for k in defaults} == defaults
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")),
+                    reason="needs nvcc")
+def test_engine_api_compiles_outside_the_library():
+    """An application with its own functors (tests/cpp/user_max_label.cu)
+    compiles against include/polymer_b200_engine.cuh and links with the
+    library: every engine symbol it needs is exported."""
+    import sys
+    import polymer_b200
+    if not os.path.exists(polymer_b200.LIB_PATH):
+        from polymer_b200 import _build
+        _build.build()
+    sys.path.insert(0, os.path.join(ROOT, "tests", "cpp"))
+    import build
+    so = build.build()
+    L = C.CDLL(so)
+    assert hasattr(L, "user_max_label")
