@@ -268,7 +268,9 @@ void apply_tunables(pm_graph *g, int32_t old_heavy_deg) {
   const GraphView &v = g->E.g;
   const size_t pbytes = (size_t)std::max(std::max(v.in.nchunks, v.out.nchunks), 1) * 16;
   if (g->partials.bytes < pbytes) g->partials.alloc(pbytes);
+  if (g->hdone.bytes < pbytes / 4) g->hdone.alloc(pbytes / 4);
   g->E.partials = g->partials.p;
+  g->E.hdone = g->hdone.as<int32_t>();
   PM_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -324,12 +326,14 @@ void finish_graph(pm_graph *g) {
   g->hubs.alloc((size_t)kMaxHubs * 4);
   // partial sums of heavy chunks, for pulls over the CSC or over the CSR
   g->partials.alloc((size_t)std::max(std::max(v.in.nchunks, v.out.nchunks), 1) * 16);
+  g->hdone.alloc((size_t)std::max(std::max(v.in.nchunks, v.out.nchunks), 1) * 4);
   g->cnt.alloc(3 * sizeof(Counters));
   PM_CUDA(cudaMemsetAsync(g->cnt.p, 0, 3 * sizeof(Counters), st));  // error words start clear
   g->E.d_cnt = g->cnt.as<Counters>();
   g->E.defer = g->defer.as<int32_t>();
   g->E.hubs = g->hubs.as<int32_t>();
   g->E.partials = g->partials.p;
+  g->E.hdone = g->hdone.as<int32_t>();
   PM_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -75,7 +75,7 @@ struct pm_graph {
   pm::DevBuf w_f32_pair_in;   // {CSC source, float weight} per CSC slot, built on first use
   pm::DevBuf w_f32_pair_out;  // {CSR destination, float weight} per CSR slot, likewise
   pm::Engine E;
-  pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials;
+  pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials, hdone;
   pm::Counters *h_cnt = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<pm::DevBuf> scratch;  // per-call workspaces kept across calls

@@ -495,9 +495,60 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f
   }
 }
 
+// One heavy chunk summed by one warp (the fused pull below): lane-strided
+// loads, 4 per lane in flight, a warp reduction, the partial published with
+// a fence and counted in done[hfirst[r]] for the row's committing lane.
 template <class F, class W>
+__device__ __forceinline__ void warp_heavy_chunk(const GraphView &g, const F &f, const W *w, int c,
+                                                 typename F::Acc *partials, int32_t *done) {
+  using Acc = typename F::Acc;
+  const int lane = lane_id();
+  const int r = __ldg(g.in.hrow + c);
+  const int first = __ldg(g.in.hfirst + r);
+  const int64_t e0 = (int64_t)__ldg(g.in.off + r) + (int64_t)(c - first) * kChunkEdges;
+  const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.in.off + r + 1));
+  Acc acc = f.identity();
+  if (f.cond(r)) {
+    constexpr int U = 4;  // loads in flight per lane (the kernel's register cap)
+    for (int64_t base = e0; base < e1; base += 32 * U) {
+      int src[U];
+      typename EdgeT<W>::type wv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t e = base + 32 * u + lane;
+        src[u] = e < e1 ? load_src(g.in.idx, w, e, wv[u]) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t e = base + 32 * u + lane;
+        if (e < e1) acc = f.combine(acc, f.edge(src[u], r, edge_w(w, e, wv[u])));
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) acc = f.combine(acc, shfl_down(acc, d));
+  if (lane == 0) {
+    partials[c] = acc;
+    __threadfence();
+    atomicAdd(done + first, 1);
+  }
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int32_t *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+constexpr int kHeavyWaitSpins = 1 << 22;  // x ~256 ns: gives up after about a second
+
+// hdone == nullptr: the partials of the heavy rows were summed by
+// k_heavy_reduce before this launch.  Otherwise (fused) the first
+// g.in.nchunks tickets are heavy chunks, summed here by warp_heavy_chunk, and
+// a heavy row's lane waits (bounded) for its chunks before it commits: every
+// chunk ticket precedes every group ticket, so its warp is already running.
+template <class F, class W, bool FUSED = false>
 __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
-                                                     const typename F::Acc *__restrict__ partials,
+                                                     typename F::Acc *partials, int32_t *hdone,
                                                      uint32_t *__restrict__ next, Counters *cnt) {
   using Acc = typename F::Acc;
   constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges, NW = kPullBlock / 32;
@@ -515,6 +566,13 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
   int grp = 0;
   if (lane == 0) grp = (int)atomicAdd(&cnt->aux, 1ull);
   grp = __shfl_sync(0xffffffffu, grp, 0);
+  if constexpr (FUSED) {
+    if (grp < g.in.nchunks) {
+      warp_heavy_chunk(g, f, w, grp, partials, hdone);
+      continue;
+    }
+    grp -= g.in.nchunks;
+  }
   if (grp >= g.in.ngroups) break;
   const int r_begin = __ldg(g.in.gstart + grp), r_end = __ldg(g.in.gstart + grp + 1);
   for (int rb = r_begin; rb < r_end; rb += 32) {
@@ -646,7 +704,19 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
     if (live && heavy) {
       const int first = __ldg(g.in.hfirst + r);
       const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
-      for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);
+      if constexpr (FUSED) {
+        int spins = 0;
+        while (ld_acquire_gpu(hdone + first) < nch) {
+          if (++spins > kHeavyWaitSpins) {
+            atomicOr(&cnt->err, (unsigned)kErrTimeout);
+            break;
+          }
+          __nanosleep(256);
+        }
+        for (int k = 0; k < nch; ++k) acc = f.combine(acc, __ldcg(partials + first + k));
+      } else {
+        for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);
+      }
     }
     const bool act = live && f.commit(r, acc, my_aux);
     const unsigned word = __ballot_sync(0xffffffffu, act);
@@ -925,6 +995,7 @@ struct Tunables {
   int32_t pull_ctas_per_sm = 0;      // persistent pull-reduce CTAs per SM (0 = occupancy limit)
   int32_t bfs_div = 20, cc_div = 8, bf_div = 20;  // default threshold = m / div
   int32_t cuda_graphs = 1;           // capture the fixed-iteration loops
+  int32_t fused_heavy = 0;           // heavy chunks summed inside the pull-reduce launch
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
@@ -965,6 +1036,7 @@ struct Engine {
   int32_t *defer = nullptr;    // n
   int32_t *hubs = nullptr;     // kMaxHubs
   void *partials = nullptr;    // max(in.nchunks, 1) * 16 bytes
+  int32_t *hdone = nullptr;    // max(in.nchunks, 1) chunk counters of the fused pull
   int num_sms = 148;
   Profiler prof;
   Tunables tune;
@@ -1130,19 +1202,29 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
   static_assert(sizeof(typename F::Acc) <= 16, "accumulator larger than the partials slot");
   using Acc = typename F::Acc;
   Acc *partials = reinterpret_cast<Acc *>(E.partials);
-  if (E.g.in.nchunks > 0)
+  const bool fused = E.tune.fused_heavy && E.g.in.nchunks > 0;
+  if (fused)
+    PM_CUDA(cudaMemsetAsync(E.hdone, 0, (size_t)E.g.in.nchunks * 4, E.stream));
+  else if (E.g.in.nchunks > 0)
     PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in,
               partials);
   // persistent grid: as many CTAs as fit on the device at once
-  static int per_sm = 0;
+  static int per_sm = 0, per_sm_fused = 0;
   if (per_sm == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull_reduce<F, W>, kPullBlock, 0));
-    if (per_sm < 1) per_sm = 1;
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull_reduce<F, W, false>, kPullBlock, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fused, k_pull_reduce<F, W, true>, kPullBlock,
+                                                          0));
+    per_sm = std::max(per_sm, 1);
+    per_sm_fused = std::max(per_sm_fused, 1);
   }
-  const int64_t want = ((int64_t)E.g.in.ngroups + kPullBlock / 32 - 1) / (kPullBlock / 32);
-  const int grid = E.persistent_grid(want, per_sm);
-  PM_LAUNCH((k_pull_reduce<F, W>), grid, kPullBlock, 0, E.stream, E.g, f, w_in, (const Acc *)partials,
-            next_bits, cnt);
+  const int64_t tickets = (int64_t)E.g.in.ngroups + (fused ? E.g.in.nchunks : 0);
+  const int64_t want = (tickets + kPullBlock / 32 - 1) / (kPullBlock / 32);
+  if (fused)
+    PM_LAUNCH((k_pull_reduce<F, W, true>), E.persistent_grid(want, per_sm_fused), kPullBlock, 0, E.stream, E.g, f,
+              w_in, partials, E.hdone, next_bits, cnt);
+  else
+    PM_LAUNCH((k_pull_reduce<F, W, false>), E.persistent_grid(want, per_sm), kPullBlock, 0, E.stream, E.g, f,
+              w_in, partials, (int32_t *)nullptr, next_bits, cnt);
 }
 
 // edgeMap (polymer.h:2240-2309): sparse push below the threshold, otherwise

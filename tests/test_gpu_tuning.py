@@ -55,21 +55,31 @@ def test_cuda_graphs_profile_counts_passes(pm):
         assert g.profile_read("pagerank", reset=True)[1] == 5
 
 
+@pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("heavy", [64, 1024, 4096, 1 << 30])
-def test_heavy_degree_results_unchanged(pm, oracle, heavy):
+def test_heavy_degree_results_unchanged(pm, oracle, heavy, fused):
     og = oracle.rmat_graph(14, 16)
     ref = oracle.pagerank(og, 10)
     sym = oracle.rmat_graph(13, 16, symmetric=True)
     w = oracle.weights_int(sym)
     srcs = oracle.pick_sources(sym, 3, seed=0x5EED0021)
     with pm.Graph.from_csr(og.off, og.idx) as g:
+        g.set_tunable("fused_heavy", fused)
         g.set_tunable("heavy_deg", heavy)
         assert g.get_tunable("heavy_deg") == heavy
         assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
+        a = pm.PageRank(g, 10, dtype=np.float64)
+        assert np.allclose(a, oracle.pagerank(og, 10), rtol=1e-10, atol=0)
+        g.gen_weights_unit()
+        x0 = oracle.uniform01(og.n)
+        ys = oracle.spmv(og, oracle.weights_unit(og).astype(np.float64), x0.astype(np.float64), 5)
+        assert rel_l1(pm.SPMV(g, x0, 5), ys) < RL1_F32
+        assert np.array_equal(pm.SPMV(g, x0, 5), pm.SPMV(g, x0, 5))   # fixed reduction order
         g.set_tunable("heavy_deg", 2048)
         assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
     with pm.Graph.from_csr(sym.off, sym.idx, symmetric=True) as g:
         g.set_weights(w)
+        g.set_tunable("fused_heavy", fused)
         g.set_tunable("heavy_deg", heavy)
         assert np.array_equal(pm.Components(g), oracle.cc(sym))
         for s in srcs:
