@@ -370,10 +370,11 @@ PM_API pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value);
 PM_API pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value);
 
 /* Autotuner: coordinate descent over the tunables application `app` uses
- * (candidates per tunable, each timed twice after a warm-up on the graph's
- * stream with CUDA events, a change kept when it saves more than 2 %); the
- * winners stay set on the handle.  PageRank / SpMV / BP time 3 iterations
- * (SpMV needs float weights), BFS four fixed sources, CC one run,
+ * (candidates per tunable, each timed three times after a warm-up on the
+ * graph's stream with CUDA events, the fastest run counting, a change kept
+ * when it saves more than 2 %); the winners stay set on the handle.
+ * PageRank / SpMV / BP time 3 iterations (SpMV needs float weights), BFS
+ * eight fixed sources, CC one run,
  * BellmanFord one source (needs int32 weights). */
 #define PM_APP_PAGERANK 0
 #define PM_APP_SPMV 1

@@ -155,7 +155,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
       break;
     }
     case PM_APP_BFS: {
-      const std::vector<int32_t> srcs = tune_sources(g, 4);
+      const std::vector<int32_t> srcs = tune_sources(g, 8);
       int32_t *p = (int32_t *)slot(5, (size_t)n * 4);
       int32_t *d = (int32_t *)slot(6, (size_t)n * 4);
       runs.push_back([=] {
@@ -208,7 +208,7 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
   auto time_once = [&] {
     run();  // warm-up: first touch, graph capture
     float best = 1e30f;
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < 3; ++r) {
       PM_CUDA(cudaEventRecord(a, E.stream));
       run();
       PM_CUDA(cudaEventRecord(b, E.stream));
