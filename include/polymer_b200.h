@@ -395,6 +395,20 @@ PM_API pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report);
  * was tuned last. */
 PM_API pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report);
 
+/* Device-memory cache.  The library allocates its device buffers through a
+ * per-process cache: a freed buffer (a graph's arrays after
+ * pm_graph_destroy, build temporaries, grown workspaces) stays reserved and
+ * is handed to a later request of close size, after a device
+ * synchronisation, instead of going through cudaFree / cudaMalloc.
+ * max_bytes: -1 (default) caps the cache at a quarter of the device's
+ * memory, 0 turns it off, > 0 caps it there; lowering the cap below what is
+ * cached releases everything.  Memory held by the cache is not available to
+ * other allocators in the process (a framework's own caching allocator, for
+ * example) until released.  No reference counterpart. */
+PM_API pm_status pm_set_memory_cache(int64_t max_bytes);
+PM_API pm_status pm_release_memory_cache(void);
+PM_API pm_status pm_memory_cache_info(int64_t *cached_bytes);
+
 /* Pinned (page-locked) host memory for fast host<->device staging. */
 PM_API pm_status pm_host_alloc(uint64_t bytes, void **out);
 PM_API pm_status pm_host_free(void *p);

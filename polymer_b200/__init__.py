@@ -122,6 +122,9 @@ def lib():
         "pm_host_free": [vp],
         "pm_graph_set_tunable": [vp, C.c_int, i64],
         "pm_graph_load_pbbs": [C.c_char_p, u32, C.c_int, C.POINTER(vp)],
+        "pm_set_memory_cache": [i64],
+        "pm_release_memory_cache": [],
+        "pm_memory_cache_info": [C.POINTER(i64)],
         "pm_graph_get_tunable": [vp, C.c_int, C.POINTER(i64)],
         "pm_tune": [vp, C.c_int, C.POINTER(TuneReport)],
         "pm_tune_mix": [vp, vp, C.c_int, C.POINTER(TuneReport)],
@@ -152,6 +155,21 @@ def get_default_tunable(name: str) -> int:
     v = C.c_int64()
     _check(lib().pm_graph_get_tunable(None, TUNABLES[name], C.byref(v)))
     return v.value
+
+
+def set_memory_cache(max_bytes: int = -1) -> None:
+    """Cap of the library's device-memory cache (-1: a quarter of the device, 0: off)."""
+    _check(lib().pm_set_memory_cache(int(max_bytes)))
+
+
+def memory_cached() -> int:
+    v = C.c_int64()
+    _check(lib().pm_memory_cache_info(C.byref(v)))
+    return v.value
+
+
+def release_memory_cache() -> None:
+    _check(lib().pm_release_memory_cache())
 
 
 def kernel_launches(reset: bool = False) -> int:

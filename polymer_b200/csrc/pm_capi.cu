@@ -48,6 +48,9 @@ void run_spmv_backward(pm_graph *g, const float *d_x, const float *d_gy, float *
 void gen_weights_lognormal(pm_graph *g, uint64_t seed);
 void set_parts(pm_graph *g, const std::vector<int64_t> &vbase);
 void set_tunable(pm_graph *g, int key, int64_t value);
+void set_memory_cache(int64_t limit);
+void release_memory_cache();
+int64_t memory_cached();
 Tunables default_tunables();
 int64_t get_tunable(pm_graph *g, int key);
 void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep);
@@ -770,6 +773,21 @@ pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *r
     need(apps != nullptr, "null apps");
     tune(g, apps, count, report);
     finish(g);
+  });
+}
+
+pm_status pm_set_memory_cache(int64_t max_bytes) {
+  return guard([&] { set_memory_cache(max_bytes); });
+}
+
+pm_status pm_release_memory_cache(void) {
+  return guard([&] { release_memory_cache(); });
+}
+
+pm_status pm_memory_cache_info(int64_t *cached_bytes) {
+  return guard([&] {
+    need(cached_bytes != nullptr, "null cached_bytes");
+    *cached_bytes = memory_cached();
   });
 }
 

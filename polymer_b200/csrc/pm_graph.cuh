@@ -8,10 +8,18 @@
 
 namespace pm {
 
+// Device memory of the library, through a per-process cache of freed blocks
+// (pm_set_memory_cache): dev_alloc returns a block of at least `bytes`
+// (*cap: its size), reusing a cached block of close size after a device
+// synchronisation (its last user's kernels may still be in flight);
+// dev_free caches the block, or frees it when the cache is full or off.
+PM_CXX_API void *dev_alloc(size_t bytes, size_t *cap);
+PM_CXX_API void dev_free(void *p, size_t cap);
+
 // Owning device buffer.
 struct DevBuf {
   void *p = nullptr;
-  size_t bytes = 0;
+  size_t bytes = 0;  // capacity (at least what alloc asked for)
   DevBuf() = default;
   explicit DevBuf(size_t b) { alloc(b); }
   DevBuf(const DevBuf &) = delete;
@@ -25,18 +33,10 @@ struct DevBuf {
   ~DevBuf() { reset(); }
   void alloc(size_t b) {
     reset();
-    if (b == 0) b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e != cudaSuccess) {
-      (void)cudaGetLastError();
-      p = nullptr;
-      fail(PM_ERR_OOM, "cudaMalloc of " + std::to_string(b) + " bytes failed: " +
-                           cudaGetErrorString(e));
-    }
-    bytes = b;
+    p = dev_alloc(b ? b : 16, &bytes);
   }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, bytes);
     p = nullptr;
     bytes = 0;
   }

@@ -96,3 +96,11 @@ def test_engine_api_compiles_outside_the_library():
     so = build.build()
     L = C.CDLL(so)
     assert hasattr(L, "user_max_label")
+
+
+def test_memory_cache_settings_host_only():
+    import polymer_b200 as pm
+    pm.set_memory_cache(1 << 30)
+    pm.set_memory_cache(-1)
+    assert pm.memory_cached() == 0  # nothing allocated without a GPU
+    pm.release_memory_cache()
