@@ -293,8 +293,7 @@ def e2e_run(pm, suite, steps):
         t0 = time.perf_counter()
         e = 0
         use_tunables(pm, suite.A)
-        with pm.Graph.from_csr(hA["off"].array, hA["idx"].array, symmetric=True) as gA:
-            gA.set_weights(hA["w"].array)
+        with pm.Graph.from_csr(hA["off"].array, hA["idx"].array, symmetric=True, weights=hA["w"].array) as gA:
             t1 = time.perf_counter()
             for k, s in enumerate(suite.sources):
                 _, _, st = pm.BFS(s, gA, stats=True, out=(oA["par"][k].array, oA["dep"][k].array))
@@ -305,8 +304,7 @@ def e2e_run(pm, suite, steps):
             t2 = time.perf_counter()
         t3 = time.perf_counter()
         use_tunables(pm, suite.B)
-        with pm.Graph.from_csr(hB["off"].array, hB["idx"].array) as gB:
-            gB.set_weights(hB["w"].array)
+        with pm.Graph.from_csr(hB["off"].array, hB["idx"].array, weights=hB["w"].array) as gB:
             t4 = time.perf_counter()
             pm.PageRank(gB, 20, dtype=np.float32, out=oB["rank"].array)
             pm.SPMV(gB, hB["x0"].array, 10, out=oB["y"].array)

@@ -59,6 +59,7 @@ typedef struct pm_graph pm_graph;
 /* value types */
 #define PM_F32 0
 #define PM_F64 1
+#define PM_I32 2
 
 /* Build a device graph from a CSR (PBBS AdjacencyGraph layout: offsets of
  * n+1 entries -- append m to the n offsets a PBBS file holds -- and m
@@ -84,6 +85,16 @@ PM_API pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, i
  * file cannot be opened. */
 #define PM_LOAD_BINARY 16u
 PM_API pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out);
+
+/* pm_graph_create with edge weights in CSR order (the weighted readers'
+ * layout, readWghGraph IO-numa.h:318-402): wtype PM_I32 (BellmanFord) or
+ * PM_F32 (SpMV).  The weights are copied on a second stream while the graph
+ * is validated and transposed, so with pinned host arrays their transfer
+ * overlaps the build; the result equals pm_graph_create followed by
+ * pm_graph_set_weights_*. */
+PM_API pm_status pm_graph_create_weighted(const int32_t *offsets, const int32_t *edges, const void *weights,
+                                          int wtype, int64_t n, int64_t m, uint32_t flags, uint32_t mem,
+                                          int device, pm_graph **out);
 
 /* Build the seeded synthetic R-MAT graph (a,b,c,d = .57,.19,.19,.05;
  * n = 2^scale, n*edge_factor draws, self loops and duplicates removed,

@@ -33,7 +33,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_
 
 PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
 PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY = 2, 4, 16
-PM_F32, PM_F64 = 0, 1
+PM_F32, PM_F64, PM_I32 = 0, 1, 2
 BF_INF = 1073741823
 
 _STATUS = {
@@ -122,6 +122,7 @@ def lib():
         "pm_host_free": [vp],
         "pm_graph_set_tunable": [vp, C.c_int, i64],
         "pm_graph_load_pbbs": [C.c_char_p, u32, C.c_int, C.POINTER(vp)],
+        "pm_graph_create_weighted": [vp, vp, vp, C.c_int, i64, i64, u32, u32, C.c_int, C.POINTER(vp)],
         "pm_set_memory_cache": [i64],
         "pm_release_memory_cache": [],
         "pm_memory_cache_info": [C.POINTER(i64)],
@@ -201,8 +202,10 @@ class Graph:
 
     @classmethod
     def from_csr(cls, offsets, edges, symmetric: bool = False, skip_self_loops: bool = False,
-                 device: int = 0) -> "Graph":
-        """offsets: n+1 int32 (offsets[n] == m); edges: m int32 destinations."""
+                 device: int = 0, weights=None) -> "Graph":
+        """offsets: n+1 int32 (offsets[n] == m); edges: m int32 destinations;
+        weights (optional): m int32 or float32 in CSR order, uploaded while
+        the graph is built."""
         n = len(offsets) - 1
         m = len(edges)
         po, mem, ko = _arg(offsets, np.int32)
@@ -211,7 +214,16 @@ class Graph:
             raise PolymerError(1, "offsets and edges must live in the same memory space")
         flags = (PM_GRAPH_SYMMETRIC if symmetric else 0) | (PM_GRAPH_SKIP_SELF_LOOPS if skip_self_loops else 0)
         h = C.c_void_p()
-        _check(lib().pm_graph_create(po, pe, n, m, flags, mem, device, C.byref(h)))
+        if weights is None:
+            _check(lib().pm_graph_create(po, pe, n, m, flags, mem, device, C.byref(h)))
+        else:
+            is_float = (np.asarray(weights).dtype.kind == "f") if not _is_device(weights) \
+                else weights.is_floating_point()
+            pw, mem3, kw = _arg(weights, np.float32 if is_float else np.int32)
+            if mem3 != mem:
+                raise PolymerError(1, "weights must live with offsets and edges")
+            _check(lib().pm_graph_create_weighted(po, pe, pw, PM_F32 if is_float else PM_I32, n, m, flags, mem,
+                                                  device, C.byref(h)))
         return cls(h)
 
     @classmethod

@@ -169,6 +169,64 @@ pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t 
   });
 }
 
+pm_status pm_graph_create_weighted(const int32_t *offsets, const int32_t *edges, const void *weights, int wtype,
+                                   int64_t n, int64_t m, uint32_t flags, uint32_t mem, int device,
+                                   pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
+    need(m >= 0 && m < (1ll << 31) - 1, "m must be in [0, 2^31-2]");
+    need(offsets != nullptr && (m == 0 || (edges != nullptr && weights != nullptr)), "null offsets/edges/weights");
+    need(wtype == PM_F32 || wtype == PM_I32, "wtype must be PM_F32 or PM_I32");
+    check_mem(mem);
+    pm_graph *g = new_graph(device, (flags & PM_GRAPH_SYMMETRIC) != 0);
+    cudaStream_t ws = nullptr;
+    cudaEvent_t wdone = nullptr;
+    try {
+      g->n = n;
+      g->m = m;
+      g->out.off.alloc((size_t)(n + 1) * 4);
+      g->out.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+      DevBuf w((size_t)std::max<int64_t>(m, 1) * 4);
+      // the CSR first; the weights follow on a second stream while the
+      // graph is validated and transposed
+      to_device(g, g->out.off.p, offsets, (size_t)(n + 1) * 4, mem);
+      to_device(g, g->out.idx.p, edges, (size_t)m * 4, mem);
+      PM_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
+      PM_CUDA(cudaEventCreateWithFlags(&wdone, cudaEventDisableTiming));
+      PM_CUDA(cudaEventRecord(wdone, g->E.stream));
+      PM_CUDA(cudaStreamWaitEvent(ws, wdone, 0));
+      if (m)
+        PM_CUDA(cudaMemcpyAsync(w.p, weights, (size_t)m * 4,
+                                mem == PM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ws));
+      PM_CUDA(cudaEventRecord(wdone, ws));
+      const bool skip = (flags & PM_GRAPH_SKIP_SELF_LOOPS) != 0;
+      if (skip) PM_CUDA(cudaStreamWaitEvent(g->E.stream, wdone, 0));  // loops drop their weights
+      ingest_csr(g, skip, &w);
+      finish_graph(g);
+      PM_CUDA(cudaStreamWaitEvent(g->E.stream, wdone, 0));
+      if (wtype == PM_F32) {
+        g->w_f32_out = std::move(w);
+        permute_weights_f32(g);
+      } else {
+        g->w_i32_out = std::move(w);
+        permute_weights_i32(g);
+      }
+      PM_CUDA(cudaStreamSynchronize(ws));
+    } catch (...) {
+      if (ws) cudaStreamSynchronize(ws);
+      if (ws) cudaStreamDestroy(ws);
+      if (wdone) cudaEventDestroy(wdone);
+      delete g;
+      throw;
+    }
+    cudaStreamDestroy(ws);
+    cudaEventDestroy(wdone);
+    *out = g;
+  });
+}
+
 pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out) {
   return guard([&] {
     need(out != nullptr, "out is null");

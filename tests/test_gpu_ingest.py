@@ -91,3 +91,31 @@ def test_missing_files(pm, tmp_path):
     with pytest.raises(pm.PolymerError) as ei:
         pm.Graph.load_pbbs(str(tmp_path / "nothing"), binary=True)
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("device_arrays", [False, True])
+def test_create_weighted_equals_create_then_set(pm, oracle, device_arrays):
+    import torch
+    og = oracle.rmat_graph(13, 16, symmetric=True)
+    wi = oracle.weights_int(og)
+    wf = oracle.weights_unit(og)
+    s = int(oracle.pick_sources(og, 1)[0])
+    arr = (lambda a: torch.from_numpy(a).cuda()) if device_arrays else (lambda a: a)
+    for w in (wi, wf):
+        with pm.Graph.from_csr(arr(og.off), arr(og.idx), symmetric=True, weights=arr(w)) as g:
+            assert same_csr(g, og)
+            if w.dtype == np.int32:
+                assert np.array_equal(g.weights_i32(), w)
+                assert np.array_equal(pm.BellmanFord(g, s), oracle.dijkstra(og, w, s))
+            else:
+                assert np.array_equal(g.weights_f32(), w)
+
+
+def test_create_weighted_skips_loops_with_their_weights(pm):
+    off = np.array([0, 2, 4, 5], np.int32)
+    idx = np.array([0, 1, 1, 2, 0], np.int32)
+    w = np.array([7, 2, 9, 3, 4], np.int32)
+    with pm.Graph.from_csr(off, idx, skip_self_loops=True, weights=w) as g:
+        o, i = g.csr()
+        assert o.tolist() == [0, 1, 2, 3] and i.tolist() == [1, 2, 0]
+        assert g.weights_i32().tolist() == [2, 3, 4]
