@@ -352,6 +352,18 @@ def batched_block(pm, suite, reps=3):
     res = {"bfs64": {"ms": round(t, 3), "gteps": round(st["edges_visited"] / (t / 1e3) / 1e9, 2),
                      "plain_64_runs_ms": round(ms_plain, 3), "speedup_vs_plain": round(ms_plain / t, 2),
                      "graph": "symmetrised R-MAT scale %d" % int(np.log2(A.n))}}
+    # asynchronous BFS (one persistent launch, reachability + parent tree) on the same sources
+    pm.BFSAsync(src64[0], A, device_out=suite.outA, out=suite.outA)
+    ms_async, e_async = 0.0, 0
+    for s in src64[:16]:
+        A.timer_begin()
+        _, sta = pm.BFSAsync(s, A, device_out=suite.outA, out=suite.outA, stats=True)
+        ms_async += A.timer_end()
+        e_async += sta["edges_visited"]
+    res["bfs_async16"] = {"ms_per_source": round(ms_async / 16, 3),
+                          "gteps": round(e_async / (ms_async / 1e3) / 1e9, 2),
+                          "level_synchronous_ms_per_source": round(ms_plain / 64, 3),
+                          "note": "one persistent launch per source; parents form a valid tree, not a BFS tree"}
     # 64-source BellmanFord over the same graph's int32 weights (1..22)
     pm.BellmanFordMulti(src64, A, device_out=out, out=out)
     ms_multi = []

@@ -165,6 +165,19 @@ typedef struct pm_traversal_stats {
 PM_API pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
                  int64_t threshold, pm_traversal_stats *stats);
 
+/* Asynchronous BFS: reachability from src with a parent tree, in one
+ * persistent launch without level barriers.  Replaces BFS(start, GA) of
+ * numa-BFS-async-pipe.C (BFS_F 52-72 driven by edgeMapSparseAsyncPipe,
+ * polymer.h:1513-1751): each vertex is claimed by the first in-neighbour whose
+ * CAS on parents[d] succeeds, whatever its level, so parents is a valid tree
+ * over exactly the vertices pm_bfs reaches (parents[src] = src, -1 when
+ * unreached; every parent edge exists; no cycles) but not a BFS tree.
+ * stats->reached = reached vertices ("Vert visited" of the reference),
+ * stats->edges_visited = out-edges scanned.  Waits inside the kernel are
+ * bounded: PM_ERR_TIMEOUT if one runs out. */
+PM_API pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32_t mem,
+                              pm_traversal_stats *stats);
+
 /* Multi-source BFS: k <= 64 sources in one traversal, one bit per source in
  * a uint64 word per vertex (BFS_F of numa-BFS.C:59-79 with the parent CAS
  * replaced by per-source visited bits; the reference runs one BFS per

@@ -24,7 +24,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "Graph", "PolymerError", "PageRank", "BFS", "BFSMulti", "Components", "BellmanFord",
+    "Graph", "PolymerError", "PageRank", "BFS", "BFSAsync", "BFSMulti", "Components", "BellmanFord",
     "BellmanFordMulti", "PageRankDelta", "SPMV",
     "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
 ]
@@ -92,6 +92,7 @@ def lib():
         "pm_fill_uniform_f32": [vp, u64, C.c_int, vp, i64],
         "pm_bfs": [vp, i32, vp, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_bfs_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
+        "pm_bfs_async": [vp, i32, vp, u32, C.POINTER(TraversalStats)],
         "pm_bellman_ford_multi": [vp, vp, C.c_int, vp, u32, i64, C.POINTER(TraversalStats)],
         "pm_ppr": [vp, vp, C.c_int, C.c_int, C.c_double, vp, u32],
         "pm_pagerank_delta": [vp, C.c_int, C.c_double, C.c_double, C.c_int, vp, u32, i64,
@@ -423,6 +424,16 @@ def BFS(start: int, g: Graph, threshold: int = -1, device_out=None, stats: bool 
     st = TraversalStats()
     _check(lib().pm_bfs(g.handle, int(start), pp, pd, mem, int(threshold), C.byref(st)))
     return (par, dep, st.as_dict()) if stats else (par, dep)
+
+
+def BFSAsync(start: int, g: Graph, device_out=None, stats: bool = False, out=None):
+    """Reachability with a parent tree from one persistent launch
+    (numa-BFS-async-pipe.C): parents over exactly the vertices BFS reaches,
+    a valid tree but not a BFS tree."""
+    par, pp, mem = _out(device_out, g.n, np.int32, out)
+    st = TraversalStats()
+    _check(lib().pm_bfs_async(g.handle, int(start), pp, mem, C.byref(st)))
+    return (par, st.as_dict()) if stats else par
 
 
 def _multi_source(fn, sources, g: Graph, threshold, device_out, stats, out):

@@ -35,6 +35,7 @@ void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, i
                pm_traversal_stats *st);
 void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist, int64_t threshold,
                   pm_traversal_stats *st);
+void run_bfs_async(pm_graph *g, int32_t src, int32_t *d_parents, pm_traversal_stats *st);
 void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double damping, float *d_out);
 void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out);
 void generate_er_batch(pm_graph *g, int count, int64_t n_min, int64_t n_max, int avg_degree,
@@ -445,6 +446,20 @@ pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uin
     run_bfs(g, src, dp, dd, threshold < 0 ? g->m / g->E.tune.bfs_div : threshold, stats);
     if (parents) from_device(g, parents, dp, bytes, mem);
     if (depth) from_device(g, depth, dd, bytes, mem);
+    finish(g);
+  });
+}
+
+pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32_t mem, pm_traversal_stats *stats) {
+  return guard([&] {
+    enter(g);
+    check_mem(mem);
+    need(parents != nullptr, "null parents");
+    need(src >= 0 && src < g->n, "source out of range");
+    const size_t bytes = (size_t)g->n * 4;
+    int32_t *dp = mem == PM_MEM_DEVICE ? parents : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
+    run_bfs_async(g, src, dp, stats);
+    if (mem == PM_MEM_HOST) from_device(g, parents, dp, bytes, mem);
     finish(g);
   });
 }
