@@ -419,6 +419,13 @@ PM_API pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report);
  * was tuned last. */
 PM_API pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report);
 
+/* Run the handle's work on a caller's CUDA stream (a cudaStream_t of the
+ * handle's device), so that it is ordered after the caller's earlier work on
+ * that stream; NULL returns to the handle's own stream.  Calls stay
+ * synchronous: each returns once its work on the stream is done.  The
+ * reference runs on its own threads; no counterpart. */
+PM_API pm_status pm_graph_set_stream(pm_graph *g, void *stream);
+
 /* Device-memory cache.  The library allocates its device buffers through a
  * per-process cache: a freed buffer (a graph's arrays after
  * pm_graph_destroy, build temporaries, grown workspaces) stays reserved and

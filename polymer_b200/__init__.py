@@ -122,6 +122,7 @@ def lib():
         "pm_host_alloc": [u64, C.POINTER(vp)],
         "pm_host_free": [vp],
         "pm_graph_set_tunable": [vp, C.c_int, i64],
+        "pm_graph_set_stream": [vp, vp],
         "pm_graph_load_pbbs": [C.c_char_p, u32, C.c_int, C.POINTER(vp)],
         "pm_graph_create_weighted": [vp, vp, vp, C.c_int, i64, i64, u32, u32, C.c_int, C.POINTER(vp)],
         "pm_set_memory_cache": [i64],
@@ -345,6 +346,12 @@ class Graph:
         ms, cnt = C.c_double(), C.c_int64()
         _check(lib().pm_profile_read(self._h, tag.encode(), C.byref(ms), C.byref(cnt), int(reset)))
         return ms.value, cnt.value
+
+    def set_stream(self, stream=None) -> None:
+        """Run this graph's work on a torch.cuda.Stream (or a raw cudaStream_t
+        handle); None returns to the graph's own stream."""
+        h = None if stream is None else getattr(stream, "cuda_stream", stream)
+        _check(lib().pm_graph_set_stream(self._h, C.c_void_p(h) if h else None))
 
     def set_tunable(self, name: str, value: int) -> None:
         _check(lib().pm_graph_set_tunable(self._h, TUNABLES[name], int(value)))

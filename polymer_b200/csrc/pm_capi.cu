@@ -109,6 +109,7 @@ static pm_graph *new_graph(int device, bool symmetric) {
   g->E.tune = default_tunables();
   try {
     PM_CUDA(cudaStreamCreateWithFlags(&g->E.stream, cudaStreamNonBlocking));
+    g->own_stream = g->E.stream;
     PM_CUDA(cudaMallocHost(&g->h_cnt, 3 * sizeof(Counters)));
     g->E.h_cnt = g->h_cnt;
     PM_CUDA(cudaEventCreate(&g->ev0));
@@ -814,6 +815,15 @@ pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_
     if (total_ms) *total_ms = tot;
     if (passes) *passes = cnt;
     if (reset) P.totals.clear();
+  });
+}
+
+pm_status pm_graph_set_stream(pm_graph *g, void *stream) {
+  return guard([&] {
+    enter(g);
+    finish(g);  // nothing of this handle stays in flight on the old stream
+    g->E.release_graphs();  // captured loops were recorded for the old stream's work
+    g->E.stream = stream ? (cudaStream_t)stream : g->own_stream;
   });
 }
 

@@ -630,5 +630,6 @@ pm_graph::~pm_graph() {
   if (h_cnt) cudaFreeHost(h_cnt);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
-  if (E.stream) cudaStreamDestroy(E.stream);
+  if (own_stream) cudaStreamSynchronize(own_stream);
+  if (own_stream) cudaStreamDestroy(own_stream);
 }

@@ -75,6 +75,7 @@ struct pm_graph {
   pm::DevBuf w_f32_pair_in;   // {CSC source, float weight} per CSC slot, built on first use
   pm::DevBuf w_f32_pair_out;  // {CSR destination, float weight} per CSR slot, likewise
   pm::Engine E;
+  cudaStream_t own_stream = nullptr;  // created with the handle; E.stream may be a caller's
   pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials, hdone;
   pm::Counters *h_cnt = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -187,3 +187,18 @@ def test_autotuner_mix_keeps_results(pm, oracle):
     with pytest.raises(pm.PolymerError):
         with pm.Graph.rmat(10, 8) as g:
             pm._check(pm.lib().pm_tune_mix(g.handle, None, 1, None))
+
+
+def test_caller_stream(pm, oracle):
+    import torch
+    og = oracle.rmat_graph(13, 16)
+    ref = oracle.pagerank(og, 5)
+    s = torch.cuda.Stream()
+    with pm.Graph.from_csr(og.off, og.idx) as g:
+        g.set_stream(s)
+        for _ in range(3):  # runs directly, captures, replays on the caller's stream
+            assert np.allclose(pm.PageRank(g, 5), ref, rtol=1e-10, atol=0)
+        _, depth = pm.BFS(0, g)
+        g.set_stream(None)
+        assert np.allclose(pm.PageRank(g, 5), ref, rtol=1e-10, atol=0)
+        assert np.array_equal(pm.BFS(0, g)[1], depth)
