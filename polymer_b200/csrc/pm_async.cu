@@ -10,9 +10,9 @@
 // was claimed before it could claim its child) -- not a BFS tree.
 //
 // Work queue: items are (vertex, chunk) in 64 bits; a vertex with more than
-// kAsyncChunk out-edges is split in chunks.  A warp takes the next item
-// (CAS on head below tail), waits for the slot to be written, relaxes the
-// item's edges lane-strided and appends the vertices it claimed with one
+// kAsyncChunk out-edges is split in chunks.  A warp takes a ticket (the next
+// slot, one atomicAdd), waits for that slot to be written, relaxes the item's
+// edges lane-strided and appends the vertices it claimed with one
 // reservation per warp.  `outstanding` counts items enqueued and not yet
 // finished: children are counted before their parent is retired, so it
 // reaches 0 only when the traversal is complete, and every warp then exits.
@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kAsyncChunk = 2048;                 // edges of one queue item
 constexpr unsigned long long kEmptySlot = ~0ull;  // queue slot not yet written
-constexpr long long kAsyncSpins = 1ll << 24;      // x ~128 ns: about two seconds
+constexpr long long kAsyncSpins = 1ll << 22;      // x <= ~1 us: a few seconds at most
 
 struct AsyncCtl {
   unsigned long long head, tail, outstanding, reached, edges;
@@ -90,47 +90,24 @@ __global__ void __launch_bounds__(256) k_bfs_async(GraphView g, int32_t *parents
   const int lane = lane_id();
   unsigned long long my_edges = 0, my_reached = 0;
   for (;;) {
-    // lane 0 takes the next item: pos, or -1 (done) / -2 (error)
-    long long pos = -1;
-    if (lane == 0) {
-      long long spins = 0;
-      for (;;) {
-        if (*(volatile unsigned *)&ctl->err) {
-          pos = -2;
-          break;
-        }
-        const unsigned long long h = ld_volatile(&ctl->head), t = ld_volatile(&ctl->tail);
-        if (h < t) {
-          if (atomicCAS(&ctl->head, h, h + 1) == h) {
-            pos = (long long)h;
-            break;
-          }
-          continue;
-        }
-        if (ld_volatile(&ctl->outstanding) == 0) {
-          pos = -1;  // nothing queued, nothing in flight
-          break;
-        }
-        if (++spins > kAsyncSpins) {
-          atomicOr(&ctl->err, (unsigned)kErrTimeout);
-          pos = -2;
-          break;
-        }
-        __nanosleep(128);
-      }
-    }
-    pos = shfl_idx(pos, 0);
-    if (pos < 0) break;
-    // the slot is written right after its reservation; wait for it (bounded)
+    // lane 0 takes a ticket (one atomicAdd, no retry loop: thousands of warps
+    // contend for the head) and waits for the item of that slot, or for the
+    // end: outstanding == 0 means nothing is queued or in flight, so the
+    // slot will never be written.  Bounded, with backoff.
     unsigned long long item = kEmptySlot;
     if (lane == 0) {
+      const unsigned long long pos = atomicAdd(&ctl->head, 1ull);
       long long spins = 0;
-      while ((item = ld_volatile(queue + pos)) == kEmptySlot) {
+      unsigned sleep = 32;
+      for (;;) {
+        if (pos < (unsigned long long)cap && (item = ld_volatile(queue + pos)) != kEmptySlot) break;
+        if (ld_volatile(&ctl->outstanding) == 0 || *(volatile unsigned *)&ctl->err) break;
         if (++spins > kAsyncSpins) {
           atomicOr(&ctl->err, (unsigned)kErrTimeout);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(sleep);
+        if (sleep < 1024) sleep <<= 1;
       }
     }
     item = shfl_idx(item, 0);
