@@ -104,3 +104,17 @@ def test_memory_cache_settings_host_only():
     pm.set_memory_cache(-1)
     assert pm.memory_cached() == 0  # nothing allocated without a GPU
     pm.release_memory_cache()
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/polymer_b200.h compiles as C99 with -pedantic: the boundary is a
+    C ABI a cgo / JNI / ctypes host can bind."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("needs gcc")
+    src = tmp_path / "c_abi.c"
+    src.write_text('#include "polymer_b200.h"\nint main(void) { pm_graph *g = 0; (void)g; return 0; }\n')
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                        "-fsyntax-only", str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
