@@ -192,37 +192,43 @@ class Suite:
         return self.pm.uniform_f32(self.B, n, seed, open_interval=True).cpu().numpy()
 
     def step(self, per):
-        """One pass of the suite; accumulates {algo: [ms, edges]} into per."""
+        """One pass of the suite; accumulates {algo: [ms, edges, algorithmic
+        bytes]} into per.  Bytes per call: BFS 4 E_r + 12 n (E_r: out-degrees of
+        the reached vertices); CC sum over rounds of 8 E_F + 12 n and
+        BellmanFord of 12 E_F + 12 n (E_F: the round's frontier out-degrees);
+        PageRank 8 m + 32 n, SpMV 12 m + 12 n, BP 4 m + 40 n per iteration."""
         pm, A, B = self.pm, self.A, self.B
         total_ms, total_edges = 0.0, 0
+        nA, nB, mB = A.n, B.n, B.m
 
-        def rec(name, ms, edges):
+        def rec(name, ms, edges, nbytes):
             nonlocal total_ms, total_edges
-            e = per.setdefault(name, [0.0, 0])
+            e = per.setdefault(name, [0.0, 0, 0])
             e[0] += ms
             e[1] += edges
+            e[2] += nbytes
             total_ms += ms
             total_edges += edges
 
         for s in self.sources:
             A.timer_begin()
             _, _, st = pm.BFS(s, A, device_out=self.outA, stats=True)
-            rec("bfs", A.timer_end(), st["edges_visited"])
+            rec("bfs", A.timer_end(), st["edges_visited"], 4 * st["edges_visited"] + 12 * nA)
         A.timer_begin()
-        pm.Components(A, device_out=self.outA)
-        rec("cc", A.timer_end(), A.m)
+        _, st = pm.Components(A, device_out=self.outA, stats=True)
+        rec("cc", A.timer_end(), A.m, 8 * st["edges_visited"] + 12 * nA * st["rounds"])
         A.timer_begin()
-        pm.BellmanFord(A, self.sources[0], device_out=self.outA)
-        rec("bellman_ford", A.timer_end(), A.m)
+        _, st = pm.BellmanFord(A, self.sources[0], device_out=self.outA, stats=True)
+        rec("bellman_ford", A.timer_end(), A.m, 12 * st["edges_visited"] + 12 * nA * st["rounds"])
         B.timer_begin()
         pm.PageRank(B, 20, dtype=np.float32, device_out=self.outB)
-        rec("pagerank", B.timer_end(), B.m * 20)
+        rec("pagerank", B.timer_end(), mB * 20, (8 * mB + 32 * nB) * 20)
         B.timer_begin()
         pm.SPMV(B, self.x0, 10)
-        rec("spmv", B.timer_end(), B.m * 10)
+        rec("spmv", B.timer_end(), mB * 10, (12 * mB + 12 * nB) * 10)
         B.timer_begin()
         pm.BeliefPropagation(B, self.prior, 10)
-        rec("bp", B.timer_end(), B.m * 10)
+        rec("bp", B.timer_end(), mB * 10, (4 * mB + 40 * nB) * 10)
         return total_ms, total_edges
 
 
@@ -734,17 +740,10 @@ def main():
     pass_ms = pr_ms / max(pr_passes, 1)
     achieved = pass_bytes / (pass_ms / 1e3) / 1e9 if pr_passes else None
     per_algo = {}
-    algo_bytes = {  # algorithmic bytes of each application's passes
-        "pagerank": lambda: (8 * mB + 32 * nB) * 20, "spmv": lambda: (12 * mB + 12 * nB) * 10,
-        "bp": lambda: (4 * mB + 40 * nB) * 10,
-    }
-    for k, (ms, e) in per.items():
-        d = {"gteps": round(e / (ms / 1e3) / 1e9, 3), "ms_per_step": round(ms / args.steps, 3)}
-        if k in algo_bytes:
-            gbs = algo_bytes[k]() * args.steps / (ms / 1e3) / 1e9
-            d["hbm_gbs"] = round(gbs, 1)
-            d["hbm_frac"] = round(gbs / hbm, 4)
-        per_algo[k] = d
+    for k, (ms, e, nbytes) in per.items():
+        gbs = nbytes / (ms / 1e3) / 1e9
+        per_algo[k] = {"gteps": round(e / (ms / 1e3) / 1e9, 3), "ms_per_step": round(ms / args.steps, 3),
+                       "hbm_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4)}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
