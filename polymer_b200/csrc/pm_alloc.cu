@@ -67,7 +67,7 @@ void release_all(Cache &c) {
 
 }  // namespace
 
-void *dev_alloc(size_t bytes, size_t *cap) {
+void *dev_alloc(size_t bytes, size_t *cap, int *device) {
   Cache &c = cache();
   const size_t want = round_cap(bytes);
   int dev = 0;
@@ -87,6 +87,7 @@ void *dev_alloc(size_t bytes, size_t *cap) {
       c.cached -= b.cap;
       PM_CUDA(cudaDeviceSynchronize());
       *cap = b.cap;
+      *device = dev;
       return b.p;
     }
   }
@@ -105,27 +106,32 @@ void *dev_alloc(size_t bytes, size_t *cap) {
     fail(PM_ERR_OOM, "cudaMalloc of " + std::to_string(want) + " bytes failed: " + cudaGetErrorString(e));
   }
   *cap = want;
+  *device = dev;
   return p;
 }
 
-void dev_free(void *p, size_t cap) {
+void dev_free(void *p, size_t cap, int dev) {
   if (!p) return;
   Cache &c = cache();
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return;
-  }
   {
     std::lock_guard<std::mutex> lk(c.mu);
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) (void)cudaGetLastError();
+    // the cap of the block's device (measured with that device current)
+    if (cur != dev) cudaSetDevice(dev);
     const int64_t lim = limit_for(c, dev);
+    if (cur != dev && cur >= 0) cudaSetDevice(cur);
     if (lim > 0 && (int64_t)(c.cached + cap) <= lim) {
       c.free.push_back(Block{p, cap, dev});
       c.cached += cap;
       return;
     }
   }
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) (void)cudaGetLastError();
+  if (cur != dev) cudaSetDevice(dev);
   cudaFree(p);
+  if (cur != dev && cur >= 0) cudaSetDevice(cur);
   (void)cudaGetLastError();
 }
 

@@ -13,30 +13,31 @@ namespace pm {
 // (*cap: its size), reusing a cached block of close size after a device
 // synchronisation (its last user's kernels may still be in flight);
 // dev_free caches the block, or frees it when the cache is full or off.
-PM_CXX_API void *dev_alloc(size_t bytes, size_t *cap);
-PM_CXX_API void dev_free(void *p, size_t cap);
+PM_CXX_API void *dev_alloc(size_t bytes, size_t *cap, int *device);
+PM_CXX_API void dev_free(void *p, size_t cap, int device);
 
 // Owning device buffer.
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;  // capacity (at least what alloc asked for)
+  int device = 0;    // where the block lives
   DevBuf() = default;
   explicit DevBuf(size_t b) { alloc(b); }
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
-  DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes), device(o.device) { o.p = nullptr; o.bytes = 0; }
   DevBuf &operator=(DevBuf &&o) noexcept {
     reset();
-    p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0;
+    p = o.p; bytes = o.bytes; device = o.device; o.p = nullptr; o.bytes = 0;
     return *this;
   }
   ~DevBuf() { reset(); }
   void alloc(size_t b) {
     reset();
-    p = dev_alloc(b ? b : 16, &bytes);
+    p = dev_alloc(b ? b : 16, &bytes, &device);
   }
   void reset() {
-    if (p) dev_free(p, bytes);
+    if (p) dev_free(p, bytes, device);
     p = nullptr;
     bytes = 0;
   }
