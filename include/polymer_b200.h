@@ -383,10 +383,11 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       second time a handle runs the same loop (same
                                       sizes, buffers and scalars) and replayed from
                                       then on; 0: plain launches */
-#define PM_TUNE_FUSED_HEAVY 8      /* 1: the chunks of heavy rows are summed inside the
-                                      pull-reduce launch (warps take them first, a row's
-                                      lane waits for its chunks, bounded); 0 (default): a
-                                      separate launch sums them first */
+#define PM_TUNE_HEAVY_MODE 8       /* how the chunks of heavy rows are summed: 0 (default)
+                                      a launch before the pull; 1 inside the pull launch
+                                      (warps take them first, a row's lane waits for its
+                                      chunks, bounded); 2 a launch beside the pull on a
+                                      second stream, the heavy rows committed after both */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

@@ -627,6 +627,7 @@ void fill_uniform(pm_graph *g, uint64_t seed, int open, float *out, int64_t coun
 pm_graph::~pm_graph() {
   if (E.stream) cudaStreamSynchronize(E.stream);
   E.release_graphs();
+  E.release_side_stream();
   if (h_cnt) cudaFreeHost(h_cnt);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);

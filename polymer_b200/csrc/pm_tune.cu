@@ -38,7 +38,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_CC_DIV: return t.cc_div;
     case PM_TUNE_BF_DIV: return t.bf_div;
     case PM_TUNE_CUDA_GRAPHS: return t.cuda_graphs;
-    case PM_TUNE_FUSED_HEAVY: return t.fused_heavy;
+    case PM_TUNE_HEAVY_MODE: return t.heavy_mode;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -82,8 +82,8 @@ void check_tunable(int key, int64_t value) {
     case PM_TUNE_CUDA_GRAPHS:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cuda_graphs must be 0 or 1");
       break;
-    case PM_TUNE_FUSED_HEAVY:
-      if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "fused_heavy must be 0 or 1");
+    case PM_TUNE_HEAVY_MODE:
+      if (value < 0 || value > 2) fail(PM_ERR_INVALID_ARG, "heavy_mode must be 0, 1 or 2");
       break;
     default:
       fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
@@ -131,7 +131,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
     case PM_APP_PAGERANK: {
       float *out = (float *)slot(0, (size_t)n * 4);
       runs.push_back([=] { run_pagerank<float>(g, 3, 0.85, out, nullptr); });
-      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_FUSED_HEAVY, PM_TUNE_PULL_CTAS_PER_SM});
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_SPMV: {
@@ -140,7 +140,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
       float *y = (float *)slot(2, (size_t)n * 4);
       fill_uniform(g, 0x7E57ull, 0, x, n);
       runs.push_back([=] { run_spmv(g, x, 3, y, nullptr); });
-      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_FUSED_HEAVY, PM_TUNE_PULL_CTAS_PER_SM});
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BP: {
@@ -151,7 +151,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
         const float psi[4] = {0.9f, 0.1f, 0.1f, 0.9f};
         run_bp(g, prior, psi, 3, out);
       });
-      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_FUSED_HEAVY, PM_TUNE_PULL_CTAS_PER_SM});
+      add_keys({PM_TUNE_HEAVY_DEG, PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BFS: {
@@ -168,7 +168,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
       int32_t *l = (int32_t *)slot(7, (size_t)n * 4);
       runs.push_back([=] { run_cc(g, l, g->m / g->E.tune.cc_div, nullptr); });
       add_keys({PM_TUNE_CC_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
-                PM_TUNE_FUSED_HEAVY, PM_TUNE_PULL_CTAS_PER_SM});
+                PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     case PM_APP_BF: {
@@ -177,7 +177,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
       int32_t *d = (int32_t *)slot(8, (size_t)n * 4);
       runs.push_back([=] { run_bellman_ford(g, src, d, g->m / g->E.tune.bf_div, nullptr); });
       add_keys({PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND, PM_TUNE_HEAVY_DEG,
-                PM_TUNE_FUSED_HEAVY, PM_TUNE_PULL_CTAS_PER_SM});
+                PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
     default:
@@ -232,7 +232,7 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
         case PM_TUNE_HEAVY_DEG: cands = {1024, 2048, 4096, 8192, 32768}; break;
         case PM_TUNE_CTA_EXPAND: cands = {128, 256, 512, 1024, 2048}; break;
         case PM_TUNE_GRID_EXPAND: cands = {2048, 4096, 16384, 65536}; break;
-        case PM_TUNE_FUSED_HEAVY: cands = {0, 1}; break;
+        case PM_TUNE_HEAVY_MODE: cands = {0, 1, 2}; break;
         case PM_TUNE_PULL_CTAS_PER_SM:
           cands.push_back(0);
           for (int c = 1; c < occupancy; ++c) cands.push_back(c);

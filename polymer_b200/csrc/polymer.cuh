@@ -541,12 +541,14 @@ __device__ __forceinline__ int ld_acquire_gpu(const int32_t *p) {
 }
 constexpr int kHeavyWaitSpins = 1 << 22;  // x ~256 ns: gives up after about a second
 
-// hdone == nullptr: the partials of the heavy rows were summed by
-// k_heavy_reduce before this launch.  Otherwise (fused) the first
-// g.in.nchunks tickets are heavy chunks, summed here by warp_heavy_chunk, and
-// a heavy row's lane waits (bounded) for its chunks before it commits: every
-// chunk ticket precedes every group ticket, so its warp is already running.
-template <class F, class W, bool FUSED = false>
+// MODE 0: the partials of the heavy rows were summed by k_heavy_reduce
+// before this launch.  MODE 1 (fused): the first g.in.nchunks tickets are
+// heavy chunks, summed here by warp_heavy_chunk, and a heavy row's lane waits
+// (bounded) for its chunks before it commits: every chunk ticket precedes
+// every group ticket, so its warp is already running.  MODE 2 (overlapped):
+// k_heavy_reduce runs at the same time on a second stream and this kernel
+// leaves the heavy rows alone; k_heavy_commit commits them afterwards.
+template <class F, class W, int MODE = 0>
 __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
                                                      typename F::Acc *partials, int32_t *hdone,
                                                      uint32_t *__restrict__ next, Counters *cnt) {
@@ -566,7 +568,7 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
   int grp = 0;
   if (lane == 0) grp = (int)atomicAdd(&cnt->aux, 1ull);
   grp = __shfl_sync(0xffffffffu, grp, 0);
-  if constexpr (FUSED) {
+  if constexpr (MODE == 1) {
     if (grp < g.in.nchunks) {
       warp_heavy_chunk(g, f, w, grp, partials, hdone);
       continue;
@@ -701,10 +703,12 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
       __syncwarp();
     }
     Acc acc = acc_s[lane];
-    if (live && heavy) {
+    bool deferred = false;  // MODE 2: k_heavy_commit finishes this row
+    if constexpr (MODE == 2) deferred = live && heavy;
+    if (live && heavy && !deferred) {
       const int first = __ldg(g.in.hfirst + r);
       const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
-      if constexpr (FUSED) {
+      if constexpr (MODE == 1) {
         int spins = 0;
         while (ld_acquire_gpu(hdone + first) < nch) {
           if (++spins > kHeavyWaitSpins) {
@@ -718,7 +722,7 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
         for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);
       }
     }
-    const bool act = live && f.commit(r, acc, my_aux);
+    const bool act = live && !deferred && f.commit(r, acc, my_aux);
     const unsigned word = __ballot_sync(0xffffffffu, act);
     if (next && lane == 0) next[rb >> 5] = word;
     if (act) {
@@ -733,6 +737,44 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
   my_aux.x = warp_sum(my_aux.x);
   my_aux.y = warp_sum(my_aux.y);
   if (lane == 0) {
+    if (my_size) {
+      atomicAdd(&cnt->size, my_size);
+      atomicAdd(&cnt->edges, my_edges);
+    }
+    if (my_aux.x != 0.0) atomicAdd(&cnt->daux, my_aux.x);
+    if (my_aux.y != 0.0) atomicAdd(&cnt->daux2, my_aux.y);
+  }
+}
+
+// The heavy rows of an overlapped pull (MODE 2): one thread per heavy row
+// (the first chunk of each row) folds the row's partials in chunk order,
+// commits, and ORs its bit into the next frontier.
+template <class F>
+__global__ void __launch_bounds__(256) k_heavy_commit(GraphView g, F f, const typename F::Acc *partials,
+                                                     uint32_t *next, Counters *cnt) {
+  using Acc = typename F::Acc;
+  unsigned long long my_size = 0, my_edges = 0;
+  double2 my_aux = make_double2(0.0, 0.0);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.in.nchunks; c += stride) {
+    const int r = __ldg(g.in.hrow + c);
+    const int first = __ldg(g.in.hfirst + r);
+    if (c != first || !f.cond(r)) continue;
+    const int deg = __ldg(g.in.off + r + 1) - __ldg(g.in.off + r);
+    const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
+    Acc acc = f.identity();
+    for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);
+    if (f.commit(r, acc, my_aux)) {
+      if (next) atomicOr(next + (r >> 5), 1u << (r & 31));
+      my_size++;
+      my_edges += __ldg(g.out.off + r + 1) - __ldg(g.out.off + r);
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  my_aux.x = warp_sum(my_aux.x);
+  my_aux.y = warp_sum(my_aux.y);
+  if (lane_id() == 0) {
     if (my_size) {
       atomicAdd(&cnt->size, my_size);
       atomicAdd(&cnt->edges, my_edges);
@@ -995,7 +1037,8 @@ struct Tunables {
   int32_t pull_ctas_per_sm = 0;      // persistent pull-reduce CTAs per SM (0 = occupancy limit)
   int32_t bfs_div = 20, cc_div = 8, bf_div = 20;  // default threshold = m / div
   int32_t cuda_graphs = 1;           // capture the fixed-iteration loops
-  int32_t fused_heavy = 0;           // heavy chunks summed inside the pull-reduce launch
+  int32_t heavy_mode = 0;            // heavy chunks: 0 a launch before the pull, 1 inside it,
+                                     // 2 a launch beside it on a second stream
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
@@ -1037,6 +1080,8 @@ struct Engine {
   int32_t *hubs = nullptr;     // kMaxHubs
   void *partials = nullptr;    // max(in.nchunks, 1) * 16 bytes
   int32_t *hdone = nullptr;    // max(in.nchunks, 1) chunk counters of the fused pull
+  cudaStream_t side = nullptr;   // second stream of the overlapped pull (created on first use)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int num_sms = 148;
   Profiler prof;
   Tunables tune;
@@ -1070,6 +1115,22 @@ struct Engine {
                  (e & kErrRange ? " (id out of range)" : ""));
       }
     return h_cnt;
+  }
+  void ensure_side_stream() {
+    if (side) return;
+    PM_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    PM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    PM_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  }
+  void release_side_stream() {
+    if (side) {
+      cudaStreamSynchronize(side);
+      cudaStreamDestroy(side);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    side = nullptr;
+    ev_fork = ev_join = nullptr;
   }
   void drop_graph(LoopGraph &lg) {
     if (lg.exec) cudaGraphExecDestroy(lg.exec);
@@ -1202,29 +1263,41 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
   static_assert(sizeof(typename F::Acc) <= 16, "accumulator larger than the partials slot");
   using Acc = typename F::Acc;
   Acc *partials = reinterpret_cast<Acc *>(E.partials);
-  const bool fused = E.tune.fused_heavy && E.g.in.nchunks > 0;
-  if (fused)
+  const int mode = E.g.in.nchunks > 0 ? E.tune.heavy_mode : 0;
+  if (mode == 1) {
     PM_CUDA(cudaMemsetAsync(E.hdone, 0, (size_t)E.g.in.nchunks * 4, E.stream));
-  else if (E.g.in.nchunks > 0)
-    PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in,
-              partials);
-  // persistent grid: as many CTAs as fit on the device at once
-  static int per_sm = 0, per_sm_fused = 0;
-  if (per_sm == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull_reduce<F, W, false>, kPullBlock, 0));
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fused, k_pull_reduce<F, W, true>, kPullBlock,
-                                                          0));
-    per_sm = std::max(per_sm, 1);
-    per_sm_fused = std::max(per_sm_fused, 1);
+  } else if (mode == 2) {
+    E.ensure_side_stream();
+    PM_CUDA(cudaEventRecord(E.ev_fork, E.stream));
+    PM_CUDA(cudaStreamWaitEvent(E.side, E.ev_fork, 0));
+    PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.side, E.g, f, w_in, partials);
+    PM_CUDA(cudaEventRecord(E.ev_join, E.side));
+  } else if (E.g.in.nchunks > 0) {
+    PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in, partials);
   }
-  const int64_t tickets = (int64_t)E.g.in.ngroups + (fused ? E.g.in.nchunks : 0);
+  // persistent grid: as many CTAs as fit on the device at once
+  static int per_sm[3] = {0, 0, 0};
+  if (per_sm[0] == 0) {
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_pull_reduce<F, W, 0>, kPullBlock, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_pull_reduce<F, W, 1>, kPullBlock, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_pull_reduce<F, W, 2>, kPullBlock, 0));
+    for (int &x : per_sm) x = std::max(x, 1);
+  }
+  const int64_t tickets = (int64_t)E.g.in.ngroups + (mode == 1 ? E.g.in.nchunks : 0);
   const int64_t want = (tickets + kPullBlock / 32 - 1) / (kPullBlock / 32);
-  if (fused)
-    PM_LAUNCH((k_pull_reduce<F, W, true>), E.persistent_grid(want, per_sm_fused), kPullBlock, 0, E.stream, E.g, f,
+  if (mode == 1) {
+    PM_LAUNCH((k_pull_reduce<F, W, 1>), E.persistent_grid(want, per_sm[1]), kPullBlock, 0, E.stream, E.g, f,
               w_in, partials, E.hdone, next_bits, cnt);
-  else
-    PM_LAUNCH((k_pull_reduce<F, W, false>), E.persistent_grid(want, per_sm), kPullBlock, 0, E.stream, E.g, f,
+  } else if (mode == 2) {
+    PM_LAUNCH((k_pull_reduce<F, W, 2>), E.persistent_grid(want, per_sm[2]), kPullBlock, 0, E.stream, E.g, f,
               w_in, partials, (int32_t *)nullptr, next_bits, cnt);
+    PM_CUDA(cudaStreamWaitEvent(E.stream, E.ev_join, 0));
+    PM_LAUNCH((k_heavy_commit<F>), E.grid_for(E.g.in.nchunks, 256, 4), 256, 0, E.stream, E.g, f,
+              (const Acc *)partials, next_bits, cnt);
+  } else {
+    PM_LAUNCH((k_pull_reduce<F, W, 0>), E.persistent_grid(want, per_sm[0]), kPullBlock, 0, E.stream, E.g, f,
+              w_in, partials, (int32_t *)nullptr, next_bits, cnt);
+  }
 }
 
 // edgeMap (polymer.h:2240-2309): sparse push below the threshold, otherwise

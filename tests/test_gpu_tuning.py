@@ -55,7 +55,7 @@ def test_cuda_graphs_profile_counts_passes(pm):
         assert g.profile_read("pagerank", reset=True)[1] == 5
 
 
-@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("fused", [0, 1, 2])
 @pytest.mark.parametrize("heavy", [64, 1024, 4096, 1 << 30])
 def test_heavy_degree_results_unchanged(pm, oracle, heavy, fused):
     og = oracle.rmat_graph(14, 16)
@@ -64,7 +64,7 @@ def test_heavy_degree_results_unchanged(pm, oracle, heavy, fused):
     w = oracle.weights_int(sym)
     srcs = oracle.pick_sources(sym, 3, seed=0x5EED0021)
     with pm.Graph.from_csr(og.off, og.idx) as g:
-        g.set_tunable("fused_heavy", fused)
+        g.set_tunable("heavy_mode", fused)
         g.set_tunable("heavy_deg", heavy)
         assert g.get_tunable("heavy_deg") == heavy
         assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
@@ -79,7 +79,7 @@ def test_heavy_degree_results_unchanged(pm, oracle, heavy, fused):
         assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
     with pm.Graph.from_csr(sym.off, sym.idx, symmetric=True) as g:
         g.set_weights(w)
-        g.set_tunable("fused_heavy", fused)
+        g.set_tunable("heavy_mode", fused)
         g.set_tunable("heavy_deg", heavy)
         assert np.array_equal(pm.Components(g), oracle.cc(sym))
         for s in srcs:
