@@ -328,7 +328,7 @@ def e2e_run(pm, suite, steps):
     t = times[i]
     names = ["build_A", "run_A", "free_A", "build_B", "run_B", "free_B"]
     return {"value": round(edges / t / 1e9, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t, 4),
+            "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t, 4), "edges_per_step": int(edges),
             "phases_s": {k: round(v, 4) for k, v in zip(names, phases[i])},
             "timing": "host clock around synchronous API calls, median of %d steps" % steps}
 
@@ -785,7 +785,14 @@ def main():
         line["adjoint"] = adjoint_block(pm, torch, suite.dev)
         line["ingest"] = ingest_block(pm)
     if not args.no_e2e:
-        line["e2e"] = e2e_run(pm, suite, args.e2e_steps)
+        e2e = e2e_run(pm, suite, args.e2e_steps)
+        if dist:  # whole job: every rank's edges over the slowest rank's step
+            ms_max, edges_all = aggregate_ranks(dist, 1e3 * e2e["seconds_per_step"], e2e["edges_per_step"], "cuda")
+            e2e.update(value=round(edges_all / (ms_max / 1e3) / 1e9, 4), seconds_per_step=round(ms_max / 1e3, 4),
+                       edges_per_step=int(edges_all), h2d_bytes_per_step=e2e["h2d_bytes_per_step"] * world,
+                       d2h_bytes_per_step=e2e["d2h_bytes_per_step"] * world,
+                       ranks="sum over %d ranks of edges and bytes, max over ranks of the step time" % world)
+        line["e2e"] = e2e
     if dist:
         dist.barrier()
         dist.destroy_process_group()

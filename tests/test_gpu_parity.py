@@ -462,6 +462,29 @@ def test_empty_and_single_vertex_graphs(pm, oracle):
         assert (d >= 0).sum() == 1
 
 
+def test_edgeless_graph_all_paths(pm, tmp_path):
+    """Every path on 100 vertices and no edges: the batched, asynchronous,
+    PageRankDelta, weighted and ingest paths included."""
+    n = 100
+    off = np.zeros(n + 1, np.int32)
+    none = np.zeros(0, np.int32)
+    with pm.Graph.from_csr(off, none, weights=none) as g:
+        srcs = [3, 50, 99]
+        assert np.array_equal(pm.BFSMulti(srcs, g), np.where(np.arange(n)[None, :] == np.array(srcs)[:, None], 0, -1))
+        d = pm.BellmanFordMulti(srcs, g)
+        assert np.array_equal(d, np.where(np.arange(n)[None, :] == np.array(srcs)[:, None], 0, pm.BF_INF))
+        par, st = pm.BFSAsync(7, g, stats=True)
+        assert st["reached"] == 1 and (par >= 0).sum() == 1 and par[7] == 7
+        p = pm.PageRankDelta(g, 3, dtype=np.float64)
+        assert np.allclose(p, 0.15 / n)  # first round: (1-d)/n; later rounds: no in-edges
+        x = pm.PersonalizedPageRank(g, [0, 5], 4)
+        assert np.allclose(x[0, 0], 0.15) and np.allclose(x[5, 1], 0.15) and x.sum() == pytest.approx(0.3, rel=1e-6)
+    path = tmp_path / "none.adj"
+    path.write_text("AdjacencyGraph\n%d\n0\n" % n + "0\n" * n)
+    with pm.Graph.load_pbbs(str(path)) as g:
+        assert g.n == n and g.m == 0
+
+
 def test_device_pointers_roundtrip(pm, oracle):
     import torch
     og = oracle.rmat_graph(12, 16, symmetric=True)
