@@ -202,3 +202,22 @@ def test_caller_stream(pm, oracle):
         g.set_stream(None)
         assert np.allclose(pm.PageRank(g, 5), ref, rtol=1e-10, atol=0)
         assert np.array_equal(pm.BFS(0, g)[1], depth)
+
+
+def test_heavy_mode_overlapped_is_bit_identical(pm):
+    """Mode 2 sums the same chunks with the same kernel on a second stream and
+    folds them in the same order: results equal mode 0 bit for bit, with and
+    without CUDA-graph capture (the fork/join of the two streams is captured)."""
+    with pm.Graph.rmat(15, 16) as g:
+        g.gen_weights_unit()
+        g.set_tunable("heavy_deg", 256)
+        x0 = pm.uniform_f32(g, g.n, 21).cpu().numpy()
+        prior = pm.uniform_f32(g, 2 * g.n, 22, open_interval=True).cpu().numpy()
+        base = _fp_runs(pm, g, x0, prior)
+        g.set_tunable("heavy_mode", 2)
+        for graphs in (1, 0):
+            g.set_tunable("cuda_graphs", graphs)
+            for _ in range(3):
+                got = _fp_runs(pm, g, x0, prior)
+                for a, b in zip(base, got):
+                    assert np.array_equal(a, b)
