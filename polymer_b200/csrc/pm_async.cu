@@ -166,11 +166,11 @@ void run_bfs_async(pm_graph *g, int32_t src, int32_t *d_parents, pm_traversal_st
   auto *ctl = (AsyncCtl *)g->scratch_buf(1, sizeof(AsyncCtl));
   PM_LAUNCH(k_async_init, E.grid_for(std::max(cap, n), 256, 16), 256, 0, E.stream, queue, cap, d_parents, n, src);
   PM_LAUNCH(k_async_seed, 1, 1, 0, E.stream, E.g, queue, src, ctl);
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_async, 256, 0));
-    per_sm = std::max(per_sm, 1);
-  }
+  static const int per_sm = [] {
+    int r = 0;
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_bfs_async, 256, 0));
+    return std::max(r, 1);
+  }();
   E.prof.begin("bfs_async", E.stream);
   PM_LAUNCH(k_bfs_async, E.num_sms * per_sm, 256, 0, E.stream, E.g, d_parents, queue, cap, ctl);
   E.prof.end(E.stream);

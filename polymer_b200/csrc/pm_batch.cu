@@ -412,13 +412,16 @@ void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_
   void *tmp = g->scratch_buf(5, std::max<size_t>(tmp_bytes, 16));
   PM_LAUNCH(k_bf_multi_init, E.grid_for(n * kLanes, 256, 16), 256, 0, E.stream, dist, act, n);
   PM_LAUNCH(k_bf_multi_seed, 1, 64, 0, E.stream, d_sources, k, dist, act);
-  static int pull_per_sm = 0, push_per_sm = 0;
-  if (pull_per_sm == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pull_per_sm, k_bf_multi_pull, 256, 0));
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&push_per_sm, k_bf_multi_push, 256, 0));
-    pull_per_sm = std::max(pull_per_sm, 1);
-    push_per_sm = std::max(push_per_sm, 1);
-  }
+  static const int pull_per_sm = [] {
+    int r = 0;
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_bf_multi_pull, 256, 0));
+    return std::max(r, 1);
+  }();
+  static const int push_per_sm = [] {
+    int r = 0;
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_bf_multi_push, 256, 0));
+    return std::max(r, 1);
+  }();
   const int64_t heavy_pieces = (int64_t)E.g.in.nchunks * (kChunkEdges / kBfPiece);
   const int pull_grid = E.persistent_grid((heavy_pieces + E.g.in.ngroups + 7) / 8, pull_per_sm);
   const int32_t *w_in = g->w_i32_in.as<int32_t>(), *w_out = g->w_i32_out.as<int32_t>();
@@ -564,11 +567,11 @@ void run_ppr(pm_graph *g, const int32_t *d_seeds, int k, int iters, double dampi
   PM_CUDA(cudaMemsetAsync(c0, 0, (size_t)n * kPprCols * 4, E.stream));
   if (iters == 0) PM_CUDA(cudaMemsetAsync(d_out, 0, (size_t)n * k * 4, E.stream));
   PM_LAUNCH(k_ppr_seed, 1, 32, 0, E.stream, d_seeds, k, E.g.out.off, c0, iters == 0 ? d_out : nullptr, k);
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppr_pull, 256, 0));
-    if (per_sm < 1) per_sm = 1;
-  }
+  static const int per_sm = [] {
+    int r = 0;
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_ppr_pull, 256, 0));
+    return std::max(r, 1);
+  }();
   const int grid = E.persistent_grid(((int64_t)E.g.in.ngroups + 7) / 8, per_sm);
   E.run_loop(loop_key("ppr", iters, k, damping, c0, c1, part, d_seeds, d_out), [&] {
     float *a = c0, *b = c1;
@@ -665,14 +668,14 @@ void run_pagerank_parts(pm_graph *g, int iters, double damping, float *d_out) {
   float *pn = (float *)g->scratch_buf(1, (size_t)n * 4);
   float *c0 = (float *)g->scratch_buf(2, (size_t)n * 4);
   float *c1 = (float *)g->scratch_buf(3, (size_t)n * 4);
-  static int clusters = 0;
-  if (clusters == 0) {
+  static const int clusters = [] {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kPartCluster * 64);
     cfg.blockDim = dim3(kPartThreads);
-    PM_CUDA(cudaOccupancyMaxActiveClusters(&clusters, (void *)k_pagerank_parts, &cfg));
-    if (clusters < 1) clusters = 1;
-  }
+    int r = 0;
+    PM_CUDA(cudaOccupancyMaxActiveClusters(&r, (void *)k_pagerank_parts, &cfg));
+    return std::max(r, 1);
+  }();
   const int grid = kPartCluster * std::max(1, std::min(clusters, count));
   PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
   E.prof.begin("pagerank_parts", E.stream);

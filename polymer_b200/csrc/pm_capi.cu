@@ -70,6 +70,7 @@ enum { kSlotIn0 = 8, kSlotIn1 = 9, kSlotOut0 = 10, kSlotOut1 = 11, kSlotAux = 12
 
 template <class Fn>
 static pm_status guard(Fn &&fn) {
+  AllocScope scope(AllocCtx{});  // enter() names the call's stream
   try {
     fn();
     t_last_error.clear();
@@ -110,7 +111,8 @@ static pm_graph *new_graph(int device, bool symmetric) {
   try {
     PM_CUDA(cudaStreamCreateWithFlags(&g->E.stream, cudaStreamNonBlocking));
     g->own_stream = g->E.stream;
-    PM_CUDA(cudaMallocHost(&g->h_cnt, 3 * sizeof(Counters)));
+    set_alloc_ctx(AllocCtx{g->E.stream, false});
+    g->h_cnt = (Counters *)pinned_small_alloc(3 * sizeof(Counters));
     g->E.h_cnt = g->h_cnt;
     PM_CUDA(cudaEventCreate(&g->ev0));
     PM_CUDA(cudaEventCreate(&g->ev1));
@@ -140,6 +142,7 @@ static void check_mem(uint32_t mem) { need(mem == PM_MEM_HOST || mem == PM_MEM_D
 static void enter(pm_graph *g) {
   need(g != nullptr, "null graph handle");
   PM_CUDA(cudaSetDevice(g->device));
+  set_alloc_ctx(AllocCtx{g->E.stream, false});  // this call's buffers live in this stream's order
 }
 
 extern "C" {
@@ -824,6 +827,7 @@ pm_status pm_graph_set_stream(pm_graph *g, void *stream) {
     finish(g);  // nothing of this handle stays in flight on the old stream
     g->E.release_graphs();  // captured loops were recorded for the old stream's work
     g->E.stream = stream ? (cudaStream_t)stream : g->own_stream;
+    set_alloc_ctx(AllocCtx{g->E.stream, false});
   });
 }
 

@@ -427,8 +427,11 @@ static void keys_to_csr(pm_graph *g, DevBuf &a, DevBuf &b, int64_t nkeys, int64_
   PM_CUDA(cudaStreamSynchronize(st));
   // The sentinel (self loops) sorts last; drop it if present.
   uint64_t last = 0;
-  PM_CUDA(cudaMemcpy(&last, uniq + (nu - 1), 8, cudaMemcpyDeviceToHost));
-  const int64_t m = (last >> 32) >= (uint64_t)n ? nu - 1 : nu;
+  if (nu > 0) {
+    PM_CUDA(cudaMemcpyAsync(&last, uniq + (nu - 1), 8, cudaMemcpyDeviceToHost, st));
+    PM_CUDA(cudaStreamSynchronize(st));
+  }
+  const int64_t m = nu > 0 && (last >> 32) >= (uint64_t)n ? nu - 1 : nu;
   if (m >= (1ll << 31) - 1) fail(PM_ERR_INVALID_ARG, "graph exceeds int32 edge offsets");
   g->n = n;
   g->m = m;
@@ -628,9 +631,12 @@ pm_graph::~pm_graph() {
   if (E.stream) cudaStreamSynchronize(E.stream);
   E.release_graphs();
   E.release_side_stream();
-  if (h_cnt) cudaFreeHost(h_cnt);
+  pm::pinned_small_free(h_cnt, 3 * sizeof(pm::Counters));
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (own_stream) cudaStreamSynchronize(own_stream);
   if (own_stream) cudaStreamDestroy(own_stream);
+  // nothing of this handle is in flight: its buffers go back idle
+  saved = pm::alloc_ctx();
+  pm::set_alloc_ctx(pm::AllocCtx{nullptr, true});
 }

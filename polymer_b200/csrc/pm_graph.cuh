@@ -10,11 +10,47 @@ namespace pm {
 
 // Device memory of the library, through a per-process cache of freed blocks
 // (pm_set_memory_cache): dev_alloc returns a block of at least `bytes`
-// (*cap: its size), reusing a cached block of close size after a device
-// synchronisation (its last user's kernels may still be in flight);
-// dev_free caches the block, or frees it when the cache is full or off.
+// (*cap: its size), reusing a cached block of close size; dev_free caches
+// the block, or frees it when the cache is full or off.
+//
+// Reuse is stream-ordered.  Every C-ABI call names the stream its work runs
+// on (AllocCtx, set by the call's entry and cleared on its exit).  A block
+// freed inside a call carries an event recorded on that stream; the call
+// that takes it makes its own stream wait on the event, so two host threads
+// that run distinct handles never wait for each other's kernels.  A block
+// freed with no stream known (C++ engine users outside the C ABI) makes the
+// next taker synchronise the device first; a block freed while `idle` (a
+// handle's destructor, after its streams were synchronised) needs neither.
+struct AllocCtx {
+  cudaStream_t stream = nullptr;
+  bool idle = false;
+};
+PM_CXX_API AllocCtx alloc_ctx();
+PM_CXX_API void set_alloc_ctx(AllocCtx c);
 PM_CXX_API void *dev_alloc(size_t bytes, size_t *cap, int *device);
 PM_CXX_API void dev_free(void *p, size_t cap, int device);
+// Small pinned host blocks, reused without cudaFreeHost (which synchronises
+// the device).
+PM_CXX_API void *pinned_small_alloc(size_t bytes);
+PM_CXX_API void pinned_small_free(void *p, size_t bytes);
+
+// Sets the allocation context for the lifetime of the object, then puts the
+// previous one back.
+struct AllocScope {
+  AllocCtx saved;
+  explicit AllocScope(AllocCtx c) : saved(alloc_ctx()) { set_alloc_ctx(c); }
+  ~AllocScope() { set_alloc_ctx(saved); }
+  AllocScope(const AllocScope &) = delete;
+  AllocScope &operator=(const AllocScope &) = delete;
+};
+
+// First base of pm_graph: its destructor runs after every member's, so the
+// idle context that ~pm_graph sets (its streams are synchronised by then)
+// covers the members' frees and is undone afterwards.
+struct IdleFreeBase {
+  AllocCtx saved{};
+  ~IdleFreeBase() { set_alloc_ctx(saved); }
+};
 
 // Owning device buffer.
 struct DevBuf {
@@ -63,7 +99,7 @@ struct AdjBuf {
 
 }  // namespace pm
 
-struct pm_graph {
+struct pm_graph : pm::IdleFreeBase {
   int device = 0;
   int64_t n = 0, m = 0;
   bool symmetric = false;

@@ -47,7 +47,8 @@ int32_t &field(Tunables &t, int key) {
 // stride (the same on every call, so trials time the same work).
 std::vector<int32_t> tune_sources(pm_graph *g, int count) {
   std::vector<int32_t> off(g->n + 1);
-  PM_CUDA(cudaMemcpy(off.data(), g->out.off.p, (size_t)(g->n + 1) * 4, cudaMemcpyDeviceToHost));
+  PM_CUDA(cudaMemcpyAsync(off.data(), g->out.off.p, (size_t)(g->n + 1) * 4, cudaMemcpyDeviceToHost, g->E.stream));
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
   std::vector<int32_t> src;
   const int64_t step = std::max<int64_t>(1, g->n / (4 * count + 1));
   for (int64_t v = step / 2; v < g->n && (int)src.size() < count; v += step)

@@ -29,6 +29,7 @@
 //                                                          (edgeMapDenseForward)
 #pragma once
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
@@ -1276,13 +1277,15 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
     PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in, partials);
   }
   // persistent grid: as many CTAs as fit on the device at once
-  static int per_sm[3] = {0, 0, 0};
-  if (per_sm[0] == 0) {
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_pull_reduce<F, W, 0>, kPullBlock, 0));
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_pull_reduce<F, W, 1>, kPullBlock, 0));
-    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_pull_reduce<F, W, 2>, kPullBlock, 0));
-    for (int &x : per_sm) x = std::max(x, 1);
-  }
+  // resident CTAs per SM of each mode's kernel (thread-safe one-time init)
+  static const std::array<int, 3> per_sm = [] {
+    std::array<int, 3> r{};
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r[0], k_pull_reduce<F, W, 0>, kPullBlock, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r[1], k_pull_reduce<F, W, 1>, kPullBlock, 0));
+    PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r[2], k_pull_reduce<F, W, 2>, kPullBlock, 0));
+    for (int &x : r) x = std::max(x, 1);
+    return r;
+  }();
   const int64_t tickets = (int64_t)E.g.in.ngroups + (mode == 1 ? E.g.in.nchunks : 0);
   const int64_t want = (tickets + kPullBlock / 32 - 1) / (kPullBlock / 32);
   if (mode == 1) {
