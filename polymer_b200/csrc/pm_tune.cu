@@ -230,7 +230,7 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
     for (int key : keys) {
       std::vector<int64_t> cands;
       switch (key) {
-        case PM_TUNE_HEAVY_DEG: cands = {1024, 2048, 4096, 8192, 32768}; break;
+        case PM_TUNE_HEAVY_DEG: cands = {512, 1024, 2048, 4096, 8192, 32768}; break;
         case PM_TUNE_CTA_EXPAND: cands = {128, 256, 512, 1024, 2048}; break;
         case PM_TUNE_GRID_EXPAND: cands = {2048, 4096, 16384, 65536}; break;
         case PM_TUNE_HEAVY_MODE: cands = {0, 1, 2}; break;
