@@ -118,6 +118,39 @@ PM_API pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_ma
  * vbase[count] = n).  Rejected with PM_ERR_BAD_GRAPH if an edge crosses
  * parts. */
 PM_API pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count);
+
+/* ---- one graph over several processes (1D vertex partition) -------------
+ * Replaces the reference's NUMA split: partitionByDegree (polymer.h:131-192)
+ * cuts the vertices into ranges of about equal in-degree, and graphFilter /
+ * graphFilter2Direction (polymer.h:346-497) give each node the edges whose
+ * destination it owns.  Here each process (one per GPU) calls
+ * pm_graph_create_partition with the WHOLE CSR (as pm_graph_create /
+ * pm_graph_create_weighted; weights may be NULL) and its rank: the ranges cut
+ * the in-edges plus a per-vertex term into equal shares on 32-vertex
+ * boundaries, the same on every rank, and the handle keeps the edges whose
+ * destination lies in its own range.  Vertex state is replicated: after
+ * every pass the library calls the exchange function set with
+ * pm_graph_set_exchange, which must gather every rank's range of buf into
+ * every rank's buf:
+ *   buf holds bounds[nranks] entries of elem_bytes; rank r's range is
+ *   [bounds[r], bounds[r+1]); the call is ordered after the work queued on
+ *   `stream` (a cudaStream_t) and the work queued on it afterwards must see
+ *   the gathered buf (an NCCL allgather-v on that stream, for instance);
+ *   return 0, or nonzero to fail the running call with PM_ERR_CUDA.
+ * Every rank must run the same calls in the same order.  pm_pagerank,
+ * pm_spmv, pm_bfs, pm_components and pm_bellman_ford run on a partition and
+ * return the whole result on every rank (the optional residual / norm
+ * arrays and the statistics count this rank's rows and edges); the other
+ * application calls return PM_ERR_NOT_SUPPORTED.  nranks 1..1024. */
+typedef int (*pm_allgather_fn)(void *user, void *buf, int64_t elem_bytes, const int64_t *bounds, int nranks,
+                               void *stream);
+PM_API pm_status pm_graph_create_partition(const int32_t *offsets, const int32_t *edges, const void *weights,
+                                           int wtype, int64_t n, int64_t m, uint32_t flags, uint32_t mem,
+                                           int rank, int nranks, int device, pm_graph **out);
+PM_API pm_status pm_graph_set_exchange(pm_graph *g, pm_allgather_fn fn, void *user);
+/* rank, nranks and the nranks+1 range bounds (0, n and 1 for a whole graph);
+ * any pointer may be NULL. */
+PM_API pm_status pm_graph_partition_info(const pm_graph *g, int *rank, int *nranks, int64_t *bounds);
 /* Part offsets (count+1 entries into vbase when vbase is not NULL). */
 PM_API pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count);
 

@@ -33,6 +33,9 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_
 
 PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
 PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY = 2, 4, 16
+# Work of one row in the pull's load balance and in the partition cut rule,
+# in edges (kRowWork of the kernels).
+ROW_WORK = 4
 PM_F32, PM_F64, PM_I32 = 0, 1, 2
 BF_INF = 1073741823
 
@@ -66,6 +69,11 @@ TUNABLES = {"heavy_deg": 0, "cta_expand": 1, "grid_expand": 2, "pull_ctas_per_sm
 APPS = {"pagerank": 0, "spmv": 1, "bp": 2, "bfs": 3, "cc": 4, "bellman_ford": 5}
 
 _lib = None
+
+
+# pm_allgather_fn: (user, buf, elem_bytes, bounds[nranks+1], nranks, stream) -> 0 on success
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.c_int,
+                          C.c_void_p)
 
 
 def lib():
@@ -131,6 +139,10 @@ def lib():
         "pm_graph_get_tunable": [vp, C.c_int, C.POINTER(i64)],
         "pm_tune": [vp, C.c_int, C.POINTER(TuneReport)],
         "pm_tune_mix": [vp, vp, C.c_int, C.POINTER(TuneReport)],
+        "pm_graph_create_partition": [vp, vp, vp, C.c_int, i64, i64, u32, u32, C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(vp)],
+        "pm_graph_set_exchange": [vp, EXCHANGE_FN, vp],
+        "pm_graph_partition_info": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -227,6 +239,61 @@ class Graph:
             _check(lib().pm_graph_create_weighted(po, pe, pw, PM_F32 if is_float else PM_I32, n, m, flags, mem,
                                                   device, C.byref(h)))
         return cls(h)
+
+    @classmethod
+    def partition(cls, offsets, edges, rank: int, nranks: int, exchange, weights=None,
+                  skip_self_loops: bool = False, device: int = 0) -> "Graph":
+        """This rank's part of one graph spread over nranks processes
+        (pm_graph_create_partition): offsets/edges/weights are the WHOLE
+        CSR; exchange(buf_ptr, elem_bytes, bounds, stream_ptr) must gather
+        every rank's range [bounds[r], bounds[r+1]) of the device array at
+        buf_ptr into every rank's copy, in the order of the CUDA stream
+        stream_ptr (polymer_b200.distributed.allgather_v builds one over
+        torch.distributed)."""
+        n = len(offsets) - 1
+        m = len(edges)
+        po, mem, ko = _arg(offsets, np.int32)
+        pe, mem2, ke = _arg(edges, np.int32)
+        if mem != mem2:
+            raise PolymerError(1, "offsets and edges must live in the same memory space")
+        pw, wtype, kw = None, PM_F32, None
+        if weights is not None:
+            is_float = (np.asarray(weights).dtype.kind == "f") if not _is_device(weights) \
+                else weights.is_floating_point()
+            pw, mem3, kw = _arg(weights, np.float32 if is_float else np.int32)
+            if mem3 != mem:
+                raise PolymerError(1, "weights must live with offsets and edges")
+            wtype = PM_F32 if is_float else PM_I32
+        flags = PM_GRAPH_SKIP_SELF_LOOPS if skip_self_loops else 0
+        h = C.c_void_p()
+        _check(lib().pm_graph_create_partition(po, pe, pw, wtype, n, m, flags, mem, rank, nranks, device,
+                                               C.byref(h)))
+        g = cls(h)
+        g.set_exchange(exchange)
+        return g
+
+    def set_exchange(self, exchange) -> None:
+        """Python callable exchange(buf_ptr, elem_bytes, bounds, stream_ptr);
+        an exception in it fails the running call (PM_ERR_CUDA)."""
+        def cb(user, buf, elem_bytes, bounds, nranks, stream):
+            try:
+                exchange(buf, int(elem_bytes), [bounds[i] for i in range(nranks + 1)], stream)
+                return 0
+            except BaseException:  # the library turns nonzero into an error status
+                import traceback
+                traceback.print_exc()
+                return 1
+        self._exchange_cb = EXCHANGE_FN(cb)  # kept alive with the handle
+        _check(lib().pm_graph_set_exchange(self._h, self._exchange_cb, None))
+
+    def partition_info(self):
+        """(rank, nranks, bounds): this handle's rank and every rank's vertex
+        range [bounds[r], bounds[r+1])."""
+        r, k = C.c_int(), C.c_int()
+        _check(lib().pm_graph_partition_info(self._h, C.byref(r), C.byref(k), None))
+        b = np.zeros(k.value + 1, np.int64)
+        _check(lib().pm_graph_partition_info(self._h, None, None, b.ctypes.data_as(C.c_void_p)))
+        return r.value, k.value, b
 
     @classmethod
     def from_pbbs(cls, offsets_n, edges, **kw) -> "Graph":

@@ -55,11 +55,14 @@ void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int
     s.edges_visited += cur.edges;
     edgeMap<int>(E, cur, BFS_F{d_parents, d_depth, level}, next, threshold, DENSE_PARALLEL, nullptr,
                  nullptr, &dense);
+    part_round(g, next);  // a partition: the next frontier of every rank
     s.rounds++;
     s.dense_rounds += dense;
     s.reached += next.size;
     std::swap(cur, next);
   }
+  part_exchange(g, d_parents, 4);  // a partition: every rank's parents and depths
+  part_exchange(g, d_depth, 4);
   if (st) *st = s;
 }
 
@@ -110,6 +113,8 @@ void run_cc(pm_graph *g, int32_t *d_labels, int64_t threshold, pm_traversal_stat
     bool dense = false;
     s.edges_visited += cur.edges;
     edgeMapReduce<int>(E, cur, CC_F{d_labels, cur.bits}, next, threshold, nullptr, nullptr, &dense);
+    part_exchange(g, d_labels, 4);  // a partition: labels and frontier of every rank
+    part_round(g, next);
     s.rounds++;
     s.dense_rounds += dense;
     std::swap(cur, next);
@@ -169,6 +174,8 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
     bool dense = false;
     s.edges_visited += cur.edges;
     edgeMapReduce<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, w_out, w_in, &dense);
+    part_exchange(g, d_dist, 4);  // a partition: distances and frontier of every rank
+    part_round(g, next);
     s.rounds++;
     s.dense_rounds += dense;
     std::swap(cur, next);
@@ -242,20 +249,25 @@ void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_re
   T *pn = (T *)g->scratch_buf(1, (size_t)n * sizeof(T));
   T *c0 = (T *)g->scratch_buf(2, (size_t)n * sizeof(T));
   T *c1 = (T *)g->scratch_buf(3, (size_t)n * sizeof(T));
-  PM_LAUNCH((k_pr_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, pc, pn, c0, E.g.out.off, n);
+  // out-degrees of the whole graph (a partition's CSR holds only its own
+  // destinations' edges)
+  const int32_t *deg_off = g->is_part ? g->glob_off.as<int32_t>() : E.g.out.off;
+  PM_LAUNCH((k_pr_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, pc, pn, c0, deg_off, n);
   const T dmp = (T)damping, added = (T)((1.0 - damping) * (1.0 / (double)n));
   E.run_loop(loop_key("pagerank", (int)sizeof(T), iters, damping, pc, pn, c0, c1, d_resid), [&] {
     T *a = pc, *b = pn, *x = c0, *y = c1;
     for (int it = 0; it < iters; ++it) {
       PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
       E.prof.begin("pagerank", E.stream);
-      launch_pull_reduce<int>(E, PR_F<T>{x, y, a, b, E.g.out.off, dmp, added}, nullptr, nullptr, E.d_cnt);
+      launch_pull_reduce<int>(E, PR_F<T>{x, y, a, b, deg_off, dmp, added}, nullptr, nullptr, E.d_cnt);
       E.prof.end(E.stream);
+      part_exchange(g, y, sizeof(T));  // a partition: next contributions of every rank
       if (d_resid) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_resid + it);
       std::swap(a, b);
       std::swap(x, y);
     }
   });
+  part_exchange(g, iters % 2 ? pn : pc, sizeof(T));  // a partition: every rank's ranks
   PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? pn : pc, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice,
                           E.stream));
 }
@@ -299,6 +311,7 @@ void run_spmv(pm_graph *g, const T *d_x0, int iters, T *d_y, double *d_norm) {
       E.prof.begin("spmv", E.stream);
       launch_pull_reduce<WPair>(E, SPMV_F<T>{a, b}, w_in, nullptr, E.d_cnt);
       E.prof.end(E.stream);
+      part_exchange(g, b, sizeof(T));  // a partition: every rank's y
       if (d_norm) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_norm + it);
       std::swap(a, b);
     }

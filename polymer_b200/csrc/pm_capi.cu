@@ -139,6 +139,13 @@ static void from_device(pm_graph *g, void *dst, const void *src, size_t bytes, u
 }
 static void finish(pm_graph *g) { PM_CUDA(cudaStreamSynchronize(g->E.stream)); }
 static void check_mem(uint32_t mem) { need(mem == PM_MEM_HOST || mem == PM_MEM_DEVICE, "mem must be PM_MEM_HOST or PM_MEM_DEVICE"); }
+// The calls a partition graph serves: pm_pagerank, pm_spmv, pm_bfs,
+// pm_components, pm_bellman_ford (and the handle queries); the others need
+// the whole graph on one device.
+static void whole_graph(const pm_graph *g, const char *what) {
+  if (g->is_part) fail(PM_ERR_NOT_SUPPORTED, std::string(what) + " needs the whole graph, not a partition");
+}
+
 static void enter(pm_graph *g) {
   need(g != nullptr, "null graph handle");
   PM_CUDA(cudaSetDevice(g->device));
@@ -232,6 +239,77 @@ pm_status pm_graph_create_weighted(const int32_t *offsets, const int32_t *edges,
   });
 }
 
+pm_status pm_graph_create_partition(const int32_t *offsets, const int32_t *edges, const void *weights, int wtype,
+                                    int64_t n, int64_t m, uint32_t flags, uint32_t mem, int rank, int nranks,
+                                    int device, pm_graph **out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = nullptr;
+    need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
+    need(m >= 0 && m < (1ll << 31) - 1, "m must be in [0, 2^31-2]");
+    need(offsets != nullptr && (m == 0 || edges != nullptr), "null offsets/edges");
+    need(weights == nullptr || wtype == PM_F32 || wtype == PM_I32, "wtype must be PM_F32 or PM_I32");
+    need(nranks >= 1 && nranks <= 1024, "nranks must be in [1, 1024]");
+    need(rank >= 0 && rank < nranks, "rank out of range");
+    check_mem(mem);
+    // the edge subset of one rank is not symmetric: kept as a directed graph
+    pm_graph *g = new_graph(device, false);
+    try {
+      g->n = n;
+      g->m = m;
+      g->out.off.alloc((size_t)(n + 1) * 4);
+      g->out.idx.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+      to_device(g, g->out.off.p, offsets, (size_t)(n + 1) * 4, mem);
+      to_device(g, g->out.idx.p, edges, (size_t)m * 4, mem);
+      DevBuf w;
+      if (weights) {
+        w.alloc((size_t)std::max<int64_t>(m, 1) * 4);
+        to_device(g, w.p, weights, (size_t)m * 4, mem);
+      }
+      ingest_csr(g, (flags & PM_GRAPH_SKIP_SELF_LOOPS) != 0, weights ? &w : nullptr);
+      restrict_to_partition(g, rank, nranks, weights ? &w : nullptr);
+      finish_graph(g);
+      if (weights && wtype == PM_F32) {
+        g->w_f32_out = std::move(w);
+        permute_weights_f32(g);
+      } else if (weights) {
+        g->w_i32_out = std::move(w);
+        permute_weights_i32(g);
+      }
+      finish(g);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+pm_status pm_graph_set_exchange(pm_graph *g, pm_allgather_fn fn, void *user) {
+  return guard([&] {
+    enter(g);
+    need(g->is_part, "not a partition graph");
+    g->part_fn = fn;
+    g->part_user = user;
+  });
+}
+
+pm_status pm_graph_partition_info(const pm_graph *g, int *rank, int *nranks, int64_t *bounds) {
+  return guard([&] {
+    need(g != nullptr, "null graph handle");
+    if (rank) *rank = g->part_rank;
+    if (nranks) *nranks = g->part_count;
+    if (bounds) {
+      if (g->is_part)
+        std::copy(g->part_bounds.begin(), g->part_bounds.end(), bounds);
+      else {
+        bounds[0] = 0;
+        bounds[1] = g->n;
+      }
+    }
+  });
+}
+
 pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out) {
   return guard([&] {
     need(out != nullptr, "out is null");
@@ -312,6 +390,7 @@ pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_max, int 
 pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_set_parts");
     need(vbase != nullptr && count >= 1, "need count >= 1 part offsets");
     std::vector<int64_t> v(vbase, vbase + count + 1);
     check_parts(g, v);
@@ -331,6 +410,7 @@ pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count) {
 pm_status pm_pagerank_parts(pm_graph *g, int iters, double damping, float *ranks, uint32_t mem) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_pagerank_parts");
     check_mem(mem);
     need(ranks != nullptr, "null ranks");
     need(iters >= 0, "iters must be >= 0");
@@ -375,6 +455,7 @@ pm_status pm_graph_get_csr(pm_graph *g, int32_t *offsets, int32_t *edges, uint32
 pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_set_weights_i32");
     check_mem(mem);
     need(w != nullptr || g->m == 0, "null weights");
     g->w_i32_out.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
@@ -386,6 +467,7 @@ pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem) 
 pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_set_weights_f32");
     check_mem(mem);
     need(w != nullptr || g->m == 0, "null weights");
     g->w_f32_out.alloc((size_t)std::max<int64_t>(g->m, 1) * 4);
@@ -397,6 +479,7 @@ pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem) {
 pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_gen_weights_i32");
     need(wmax >= 1, "wmax must be >= 1");
     gen_weights(g, seed, wmax, false);
   });
@@ -405,6 +488,7 @@ pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax) {
 pm_status pm_graph_gen_weights_f32(pm_graph *g, uint64_t seed) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_gen_weights_f32");
     gen_weights(g, seed, 0, true);
   });
 }
@@ -457,6 +541,7 @@ pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uin
 pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32_t mem, pm_traversal_stats *stats) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_bfs_async");
     check_mem(mem);
     need(parents != nullptr, "null parents");
     need(src >= 0 && src < g->n, "source out of range");
@@ -487,6 +572,7 @@ pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dept
                        int64_t threshold, pm_traversal_stats *stats) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_bfs_multi");
     check_mem(mem);
     need(sources != nullptr && depth != nullptr, "null sources/depth");
     const int32_t *ds = stage_sources(g, sources, k, mem);
@@ -502,6 +588,7 @@ pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int3
                                 int64_t threshold, pm_traversal_stats *stats) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_bellman_ford_multi");
     check_mem(mem);
     need(sources != nullptr && dist != nullptr, "null sources/dist");
     need(g->w_i32_out.p != nullptr, "graph has no int32 weights (pm_graph_set_weights_i32)");
@@ -572,6 +659,7 @@ pm_status pm_pagerank_delta(pm_graph *g, int iters, double damping, double epsil
                             uint32_t mem, int64_t threshold, pm_traversal_stats *stats) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_pagerank_delta");
     check_mem(mem);
     need(ranks != nullptr, "null ranks");
     need(iters >= 1, "iters must be >= 1 (the reference loops until maxIter)");
@@ -596,6 +684,7 @@ pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, double dam
                  uint32_t mem) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_ppr");
     check_mem(mem);
     need(seeds != nullptr && out != nullptr, "null seeds/out");
     need(k >= 1 && k <= 32, "k must be in [1, 32]");
@@ -666,6 +755,7 @@ pm_status pm_weighted_pagerank(pm_graph *g, double damping, double tol, int max_
                                uint32_t mem, int *iters, double *resid) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_weighted_pagerank");
     check_mem(mem);
     need(p != nullptr, "null p");
     need(max_iters >= 1 && tol >= 0, "need max_iters >= 1 and tol >= 0");
@@ -684,6 +774,7 @@ pm_status pm_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_i
                               double *resid) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_pagerank_adjoint");
     check_mem(mem);
     need(p != nullptr && grad_p != nullptr && dw != nullptr, "null p/grad_p/dw");
     need(max_iters >= 1 && tol >= 0, "need max_iters >= 1 and tol >= 0");
@@ -708,6 +799,7 @@ pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, flo
                            uint32_t mem) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_spmv_backward");
     check_mem(mem);
     need(x != nullptr && grad_y != nullptr, "null x/grad_y");
     need_weights_f32(g);
@@ -729,6 +821,7 @@ pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, flo
 pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_graph_gen_weights_lognormal");
     gen_weights_lognormal(g, seed);
   });
 }
@@ -737,6 +830,7 @@ extern "C++" {
 template <class T>
 static void bp_call(pm_graph *g, const T *prior, const T *psi, int iters, T *log_prod, uint32_t mem) {
   enter(g);
+  whole_graph(g, "pm_bp");
   check_mem(mem);
   need(prior != nullptr && psi != nullptr && log_prod != nullptr, "null prior/psi/log_prod");
   need(iters >= 0, "iters must be >= 0");
@@ -849,6 +943,7 @@ pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
 pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_tune");
     tune(g, &app, 1, report);
     finish(g);
   });
@@ -857,6 +952,7 @@ pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
 pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report) {
   return guard([&] {
     enter(g);
+    whole_graph(g, "pm_tune_mix");
     need(apps != nullptr, "null apps");
     tune(g, apps, count, report);
     finish(g);

@@ -100,21 +100,22 @@ __global__ void k_lower_bound_offsets(const int32_t *keys, int64_t m, int64_t n,
 // Symmetric graph: CSC slot p (row d, neighbour s) -> CSR edge s->d.
 
 // ---- load-balance tables ---------------------------------------------------
-// Warp groups split the merge path of rows and edges: with the work key
-// key(r) = off[r] + kRowWork * r (strictly increasing), gstart[g] is the
-// first row whose key is >= g * kGroupWork, rounded down to a multiple of 32;
-// gstart[G] = n.  A group therefore holds about kGroupWork units of edges
-// plus rows, however the degrees are distributed.
-__global__ void k_group_starts(const int32_t *off, int64_t n, int32_t G, int32_t *gstart) {
+// Warp groups split the merge path of rows and edges over the rows [r0, r1)
+// (all rows, or a partition's own range; r0 a multiple of 32): with the work
+// key key(r) = off[r] - off[r0] + kRowWork * (r - r0) (strictly increasing),
+// gstart[g] is the first row whose key is >= g * kGroupWork, rounded down to
+// a multiple of 32; gstart[G] = r1.  A group therefore holds about
+// kGroupWork units of edges plus rows, however the degrees are distributed.
+__global__ void k_group_starts(const int32_t *off, int64_t r0, int64_t r1, int32_t G, int32_t *gstart) {
   GRID_STRIDE(g, (int64_t)G + 1) {
-    if (g == G) { gstart[g] = (int32_t)n; continue; }
-    int64_t target = g * (int64_t)kGroupWork;
-    int64_t lo = 0, hi = n;
+    if (g == G) { gstart[g] = (int32_t)r1; continue; }
+    const int64_t target = g * (int64_t)kGroupWork, base = off[r0];
+    int64_t lo = r0, hi = r1;
     while (lo < hi) {
       int64_t mid = (lo + hi) >> 1;
-      if ((int64_t)off[mid] + (int64_t)kRowWork * mid < target) lo = mid + 1; else hi = mid;
+      if ((int64_t)off[mid] - base + (int64_t)kRowWork * (mid - r0) < target) lo = mid + 1; else hi = mid;
     }
-    gstart[g] = (int32_t)(std::min<int64_t>(lo, n) & ~31ll);
+    gstart[g] = (int32_t)(std::min<int64_t>(lo, r1) & ~31ll);
   }
 }
 
@@ -232,12 +233,15 @@ static void build_heavy(pm_graph *g, AdjBuf &a, cudaStream_t st, int32_t heavy_d
   if (&a == &g->out) g->max_out_deg = maxdeg;
 }
 
-static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st) {
-  const int64_t n = g->n, m = g->m;
-  a.ngroups = (int32_t)((m + kRowWork * n + kGroupWork - 1) / kGroupWork);
+// Group and heavy tables of one adjacency; the rows [r0, r1) are the rows
+// the pulls over it visit (all rows, or a partition's own range, which holds
+// every edge of a partition's CSC).
+static void build_tables(pm_graph *g, AdjBuf &a, cudaStream_t st, int64_t r0, int64_t r1) {
+  const int64_t m = g->m;
+  a.ngroups = (int32_t)((m + kRowWork * (r1 - r0) + kGroupWork - 1) / kGroupWork);
   if (a.ngroups < 1) a.ngroups = 1;
   a.gstart.alloc((size_t)(a.ngroups + 1) * 4);
-  PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), n, a.ngroups,
+  PM_LAUNCH(k_group_starts, grid1d(a.ngroups + 1), 256, 0, st, a.off.as<int32_t>(), r0, r1, a.ngroups,
             a.gstart.as<int32_t>());
   build_heavy(g, a, st, g->E.tune.heavy_deg);
 }
@@ -277,7 +281,7 @@ void finish_graph(pm_graph *g) {
   // Source of every CSR edge (needed for the transpose and weight rules).
   DevBuf src((size_t)std::max<int64_t>(m, 1) * 4);
   fill_edge_src(g->out.off.as<int32_t>(), n, m, src.as<int32_t>(), st);
-  build_tables(g, g->out, st);
+  build_tables(g, g->out, st, 0, n);
   // Stable radix sort of (dst, edge id): sources stay ascending per row, so
   // slot p of the sorted order is the CSC slot of the edge it holds.  For a
   // symmetric graph the CSC is the CSR itself and this is the reverse-edge
@@ -305,7 +309,8 @@ void finish_graph(pm_graph *g) {
     if (m)
       PM_LAUNCH(k_gather_src, grid1d(m), 256, 0, st, src.as<int32_t>(), g->in_eid.as<int32_t>(), m,
                 g->in.idx.as<int32_t>());
-    build_tables(g, g->in, st);
+    // a partition's CSC holds only its own rows: its pulls visit only them
+    build_tables(g, g->in, st, g->is_part ? g->part_lo : 0, g->is_part ? g->part_hi : n);
   }
   // Views and workspaces.
   set_views(g);

@@ -121,6 +121,21 @@ struct pm_graph : pm::IdleFreeBase {
   // largest-first order in which persistent kernels take them
   std::vector<int64_t> parts;       // count+1 vertex offsets (host copy); empty if none
   pm::DevBuf parts_vbase, parts_order;
+  // 1D vertex partition across processes (pm_graph_create_partition): this
+  // handle holds the edges whose destination lies in [part_lo, part_hi)
+  // (rank r owns [part_bounds[r], part_bounds[r+1]); part_wbounds are the
+  // same bounds in bitmap words), the in-adjacency groups cover only those
+  // rows, and glob_off keeps the whole graph's CSR offsets (global
+  // out-degrees).  part_fn gathers every rank's range of a vertex array into
+  // every rank's copy.
+  bool is_part = false;
+  int part_rank = 0, part_count = 1;
+  int64_t part_lo = 0, part_hi = 0;
+  std::vector<int64_t> part_bounds, part_wbounds;
+  pm::DevBuf glob_off;
+  int (*part_fn)(void *user, void *buf, int64_t elem_bytes, const int64_t *bounds, int nranks,
+                 void *stream) = nullptr;
+  void *part_user = nullptr;
 
   pm::VertexSubset subset(int k) {
     pm::VertexSubset s;
@@ -151,4 +166,18 @@ void permute_weights_f32(pm_graph *g);
 // The float weights paired with their CSC source ids, or with their CSR
 // destination ids when csr (built once per weights).
 const WPair *ensure_f32_pairs(pm_graph *g, bool csr = false);
+
+// ---- 1D vertex partition (pm_partition.cu) ----
+// Splits the validated CSR's vertices into nranks ranges of about equal
+// in-edges + kRowWork * rows (the pull work of a range), every interior
+// bound a multiple of 32 (whole bitmap words); keeps the edges (and weights)
+// whose destination lies in rank's range; records the bounds and the whole
+// graph's offsets.
+void restrict_to_partition(pm_graph *g, int rank, int nranks, DevBuf *w);
+// Every rank's range of buf (n entries of elem_bytes) into every rank's
+// buf, through the handle's exchange function, in stream order.
+void part_exchange(pm_graph *g, void *buf, size_t elem_bytes);
+// After a round on a partition: the next frontier's bitmap made global, its
+// size and out-degree sum recounted.
+void part_round(pm_graph *g, VertexSubset &next);
 }  // namespace pm

@@ -1075,6 +1075,7 @@ struct LoopGraph {
 struct Engine {
   GraphView g;
   cudaStream_t stream = nullptr;
+  bool host_steps = false;     // loops call back to the host between passes: never captured
   Counters *d_cnt = nullptr;   // [0] next frontier, [1] deferred rows, [2] aux
   Counters *h_cnt = nullptr;   // pinned mirror
   int32_t *defer = nullptr;    // n
@@ -1149,7 +1150,7 @@ struct Engine {
   // the launches bake in: pointers, sizes, scalars and whether profiling is on.
   template <class Body>
   void run_loop(const std::string &key_in, Body &&body) {
-    if (!tune.cuda_graphs) {
+    if (!tune.cuda_graphs || host_steps) {
       body();
       return;
     }
