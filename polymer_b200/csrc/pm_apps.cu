@@ -41,8 +41,184 @@ __global__ void k_bfs_init(int32_t *parents, int32_t *depth, int64_t n, int32_t 
   }
 }
 
+// ---------------------------------------------------------------------------
+// BFS with its rounds driven on the GPU.  The host loop above reads the
+// frontier's size and out-degree sum back after every round to pick the next
+// round's direction (about 20 us of idle GPU per level).  Here one CUDA graph
+// holds a WHILE node whose body runs two rounds (frontier A -> B, B -> A): a
+// one-thread kernel decides each round's direction from the counters on the
+// device (the same rule, |F| + outdeg(F) >= threshold), the sparse and dense
+// kernels return at once when it is not their round, and the round's last
+// kernel updates the frontier state and ends the loop when the frontier is
+// empty.  The host synchronises once per BFS.
+struct BFS_GF {  // BFS_F with the level read from the round state
+  int32_t *parents;
+  int32_t *depth;
+  const RoundGate *gate;
+  __device__ __forceinline__ bool cond(int d) const {
+    return *((volatile int32_t *)parents + d) == -1;
+  }
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int) const {
+    if (atomicCAS(parents + d, -1, s) == -1) {
+      depth[d] = gate->level;
+      return true;
+    }
+    return false;
+  }
+};
+
+struct DevRound {
+  RoundGate gate;
+  unsigned long long rounds, dense_rounds, reached, edges_visited, slots;
+  unsigned int err, pad;
+};
+
+static_assert(sizeof(DevRound) <= 3 * sizeof(Counters), "DevRound is read back through the pinned counter words");
+
+// The frontier {src} (its bitmap word; the bitmap was cleared) and the round
+// state of a BFS from src.
+__global__ void k_round_init(DevRound *dr, uint32_t *bits, const int32_t *out_off, int32_t src) {
+  bits[src >> 5] = 1u << (src & 31);
+  dr->gate.size = 1;
+  dr->gate.edges = (unsigned long long)(out_off[src + 1] - out_off[src]);
+  dr->gate.active = 1;
+  dr->gate.dense = 0;
+  dr->gate.qsize = 1;
+  dr->gate.level = 0;
+  dr->rounds = dr->dense_rounds = dr->edges_visited = dr->slots = 0;
+  dr->reached = 1;
+  dr->err = 0;
+}
+
+// The round's direction and fresh counters (their error words are kept).
+__global__ void k_round_begin(DevRound *dr, Counters *cnt, int64_t threshold) {
+  RoundGate &g = dr->gate;
+  g.active = g.size > 0;
+  g.dense = (long long)(g.size + g.edges) >= threshold;
+  g.qsize = (int32_t)g.size;
+  if (g.active) g.level += 1;
+  for (int i = 0; i < 3; ++i) {
+    cnt[i].size = cnt[i].edges = cnt[i].aux = 0;
+    cnt[i].daux = cnt[i].daux2 = 0.0;
+  }
+}
+
+__global__ void k_round_end(DevRound *dr, const Counters *cnt, cudaGraphConditionalHandle loop,
+                            int32_t max_level) {
+  RoundGate &g = dr->gate;
+  dr->slots += 1;
+  if (g.active) {
+    dr->rounds += 1;
+    dr->dense_rounds += g.dense;
+    dr->edges_visited += g.edges;
+    dr->reached += cnt[0].size;
+    g.size = cnt[0].size;
+    g.edges = cnt[0].edges;
+  }
+  dr->err |= cnt[0].err | cnt[1].err | cnt[2].err;
+  const bool more = g.size > 0 && g.level < max_level && dr->err == 0;
+  cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+
+constexpr int kRoundKernels = 7;  // kernels of one round in the loop body
+
+static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
+                          pm_traversal_stats *st) {
+  Engine &E = g->E;
+  VertexSubset A = g->subset(0), B = g->subset(1);
+  auto *dr = (DevRound *)g->scratch_buf(30, sizeof(DevRound));
+  PM_LAUNCH(k_bfs_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_parents, d_depth, g->n, src);
+  PM_CUDA(cudaMemsetAsync(A.bits, 0, A.words() * 4, E.stream));
+  PM_LAUNCH(k_round_init, 1, 1, 0, E.stream, dr, A.bits, E.g.out.off, src);
+  char key[160];
+  std::snprintf(key, sizeof key, "bfs_rounds|%lld|%p|%p|%p", (long long)threshold, (void *)d_parents,
+                (void *)d_depth, (void *)dr);
+  LoopGraph *lg = nullptr;
+  for (auto &x : E.graphs)
+    if (x.key == key) lg = &x;
+  if (!lg) {
+    if (E.graphs.size() >= 16) {
+      E.drop_graph(E.graphs.front());
+      E.graphs.erase(E.graphs.begin());
+    }
+    LoopGraph fresh;
+    fresh.key = key;
+    cudaGraph_t graph = nullptr;
+    PM_CUDA(cudaGraphCreate(&graph, 0));
+    try {
+      cudaGraphConditionalHandle loop;
+      PM_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = loop;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      PM_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      const long long before = launches(false);
+      PM_CUDA(cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      const int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
+      const int qgrid = E.grid_for(((A.words() + 31) / 32) * 32, 256, 8);
+      const int32_t max_level = (int32_t)std::min<int64_t>(g->n + 1, 0x7ffffff0);
+      auto round = [&](VertexSubset &cur, VertexSubset &next) {
+        const BFS_GF f{d_parents, d_depth, &dr->gate};
+        const RoundGate *gate = &dr->gate;
+        PM_LAUNCH(k_round_begin, 1, 1, 0, E.stream, dr, E.d_cnt, threshold);
+        PM_CUDA(cudaMemsetAsync(next.bits, 0, next.words() * 4, E.stream));
+        PM_LAUNCH(k_bits_to_queue, qgrid, 256, 0, E.stream, cur.n, E.g.out.off, cur.bits, cur.queue, E.d_cnt + 2,
+                  gate);
+        PM_LAUNCH((k_sparse_push<BFS_GF, int>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.queue, 0, f,
+                  (const int *)nullptr, next.queue, next.bits, next.n, E.d_cnt, E.hubs, E.d_cnt + 1, gate);
+        PM_LAUNCH((k_sparse_push_hubs<BFS_GF, int>), E.num_sms * 4, 256, 0, E.stream, E.g, f, (const int *)nullptr,
+                  E.hubs, E.d_cnt + 1, next.queue, next.bits, next.n, E.d_cnt, gate);
+        PM_LAUNCH((k_dense_pull<BFS_GF, int>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, E.g, cur.bits, f,
+                  (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
+        PM_LAUNCH((k_dense_pull_defer<BFS_GF, int>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.bits, f,
+                  (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
+        PM_LAUNCH(k_round_end, 1, 1, 0, E.stream, dr, E.d_cnt, loop, max_level);
+      };
+      round(A, B);
+      round(B, A);
+      cudaGraph_t captured = nullptr;
+      PM_CUDA(cudaStreamEndCapture(E.stream, &captured));
+      count_launch((int)-(launches(false) - before));  // captured, not run
+      PM_CUDA(cudaGraphInstantiate(&fresh.exec, graph, 0));
+    } catch (...) {
+      cudaGraphDestroy(graph);
+      throw;
+    }
+    cudaGraphDestroy(graph);
+    E.graphs.push_back(std::move(fresh));
+    lg = &E.graphs.back();
+  }
+  E.prof.begin("bfs", E.stream);
+  PM_CUDA(cudaGraphLaunch(lg->exec, E.stream));
+  E.prof.end(E.stream);
+  DevRound h{};
+  PM_CUDA(cudaMemcpyAsync(E.h_cnt, dr, sizeof(DevRound), cudaMemcpyDeviceToHost, E.stream));
+  PM_CUDA(cudaStreamSynchronize(E.stream));
+  std::memcpy(&h, E.h_cnt, sizeof h);
+  count_launch((int)(kRoundKernels * h.slots));
+  if (h.err)
+    fail(h.err & kErrTimeout ? PM_ERR_TIMEOUT : PM_ERR_CUDA,
+         std::string("device error word ") + std::to_string(h.err) +
+             (h.err & kErrQueueOverflow ? " (queue overflow)" : "") + (h.err & kErrRange ? " (id out of range)" : ""));
+  if (st) {
+    *st = pm_traversal_stats{};
+    st->rounds = (int64_t)h.rounds;
+    st->dense_rounds = (int64_t)h.dense_rounds;
+    st->reached = (int64_t)h.reached;
+    st->edges_visited = (int64_t)h.edges_visited;
+  }
+}
+
 void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
              pm_traversal_stats *st) {
+  if (g->E.tune.cuda_graphs && !g->is_part) {
+    run_bfs_graph(g, src, d_parents, d_depth, threshold, st);
+    return;
+  }
   Engine &E = g->E;
   VertexSubset cur = g->subset(0), next = g->subset(1);
   PM_LAUNCH(k_bfs_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_parents, d_depth, g->n, src);

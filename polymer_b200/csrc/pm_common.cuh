@@ -129,6 +129,15 @@ struct Counters {
   unsigned int pad;
 };
 
+// Round state of a traversal whose rounds run on the GPU without the host
+// (a CUDA graph with a WHILE node): the frontier's size and out-degree sum,
+// whether this round runs at all (active), its direction and level.  The
+// frontier kernels given a gate return at once unless it is their round.
+struct RoundGate {
+  unsigned long long size, edges;  // the current frontier
+  int32_t active, dense, qsize, level;
+};
+
 enum DeviceError : unsigned int { kErrNone = 0, kErrQueueOverflow = 1, kErrRange = 2, kErrTimeout = 4 };
 
 }  // namespace pm

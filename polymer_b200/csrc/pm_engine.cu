@@ -27,7 +27,8 @@ long long launches(bool reset) {
 
 __global__ void k_bits_to_queue(int32_t n, const int32_t *__restrict__ out_off,
                                 const uint32_t *__restrict__ bits, int32_t *__restrict__ queue,
-                                Counters *cnt) {
+                                Counters *cnt, const RoundGate *gate) {
+  if (gate && (!gate->active || gate->dense)) return;  // not a sparse round
   const int lane = lane_id();
   const int64_t nw = ((int64_t)n + 31) / 32;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);

@@ -157,12 +157,17 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
                                                      int32_t *__restrict__ next_queue,
                                                      uint32_t *__restrict__ next_bits, int32_t qcap,
                                                      Counters *cnt, int32_t *__restrict__ hubs,
-                                                     Counters *hub_cnt) {
+                                                     Counters *hub_cnt, const RoundGate *gate = nullptr) {
   __shared__ int s_pos[256];
   __shared__ int s_v[256];
   __shared__ int s_o[256];
   __shared__ int s_warp_tot[8];
   __shared__ int s_owner, s_cv, s_co, s_cd;
+  if (gate) {  // a round driven on the GPU: the queue is what k_bits_to_queue
+    // wrote just before, counted in cnt[2] (cnt is the engine's counter array)
+    if (!gate->active || gate->dense) return;
+    qsize = (int32_t)min(cnt[2].size, (unsigned long long)qcap);
+  }
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   unsigned long long my_edges = 0;
   for (int64_t base = (int64_t)blockIdx.x * 256; base < qsize; base += (int64_t)gridDim.x * 256) {
@@ -263,10 +268,12 @@ __global__ void __launch_bounds__(256) k_sparse_push_hubs(GraphView g, F f, cons
                                                           const Counters *hub_cnt,
                                                           int32_t *__restrict__ next_queue,
                                                           uint32_t *__restrict__ next_bits,
-                                                          int32_t qcap, Counters *cnt) {
+                                                          int32_t qcap, Counters *cnt,
+                                                          const RoundGate *gate = nullptr) {
   constexpr int K = 8;
   __shared__ int s_pos[kMaxHubs + 1];
   __shared__ int s_warp[8];
+  if (gate && (!gate->active || gate->dense)) return;  // not a sparse round
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nh = (int)min(hub_cnt->size, (unsigned long long)kMaxHubs);
   if (nh == 0) return;
@@ -343,7 +350,8 @@ __global__ void __launch_bounds__(256) k_dense_pull(GraphView g, const uint32_t 
                                                     F f, const W *__restrict__ w,
                                                     uint32_t *__restrict__ next,
                                                     int32_t *__restrict__ defer, Counters *cnt,
-                                                    Counters *dcnt) {
+                                                    Counters *dcnt, const RoundGate *gate = nullptr) {
+  if (gate && (!gate->active || !gate->dense)) return;  // not a dense round
   const int lane = lane_id();
   unsigned long long my_edges = 0, my_size = 0;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
@@ -391,7 +399,9 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
                                                           const W *__restrict__ w,
                                                           uint32_t *__restrict__ next,
                                                           const int32_t *__restrict__ defer,
-                                                          Counters *cnt, const Counters *dcnt) {
+                                                          Counters *cnt, const Counters *dcnt,
+                                                          const RoundGate *gate = nullptr) {
+  if (gate && (!gate->active || !gate->dense)) return;  // not a dense round
   const int lane = lane_id();
   const int64_t nd = (int64_t)dcnt->size;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -875,7 +885,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_push(GraphView g,
 // compaction, one queue atomic per warp; also counts |F| and sum outdeg(F).
 __global__ void k_bits_to_queue(int32_t n, const int32_t *__restrict__ out_off,
                                 const uint32_t *__restrict__ bits, int32_t *__restrict__ queue,
-                                Counters *cnt);
+                                Counters *cnt, const RoundGate *gate = nullptr);
 // Queue -> bitmap (LocalFrontier::toDense, polymer.h:594-601).
 __global__ void k_queue_to_bits(const int32_t *__restrict__ queue, int32_t size,
                                 uint32_t *__restrict__ bits);
