@@ -421,6 +421,11 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       (warps take them first, a row's lane waits for its
                                       chunks, bounded); 2 a launch beside the pull on a
                                       second stream, the heavy rows committed after both */
+#define PM_TUNE_HUB_CACHE 9        /* FP32 PageRank: the contributions of up to this many
+                                      highest out-degree sources are kept in every SM's
+                                      shared memory during a pass (0 = off, the default; at
+                                      most 16384; results are unchanged; slower than the
+                                      plain pull on the R-MAT workloads measured) */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

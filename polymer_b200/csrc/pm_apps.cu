@@ -381,9 +381,11 @@ struct PR_F {
   const int32_t *out_off;
   T damping, added;
   using Acc = T;
+  static constexpr bool kHubs = true;  // edge() is a plain load of c_cur[s]
   __device__ __forceinline__ bool cond(int) const { return true; }
   __device__ __forceinline__ Acc identity() const { return T(-0.0); }
   __device__ __forceinline__ Acc edge(int s, int, int) const { return __ldg(c_cur + s); }
+  __device__ __forceinline__ Acc edge_value(Acc v, int, int) const { return v; }
   __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return a + b; }
   __device__ __forceinline__ bool commit(int d, Acc acc, double2 &resid) const {
     const bool in_f = !signbit(__ldg(c_cur + d));
@@ -430,12 +432,21 @@ void run_pagerank(pm_graph *g, int iters, double damping, T *d_out, double *d_re
   const int32_t *deg_off = g->is_part ? g->glob_off.as<int32_t>() : E.g.out.off;
   PM_LAUNCH((k_pr_init<T>), E.grid_for(n, 256, 16), 256, 0, E.stream, pc, pn, c0, deg_off, n);
   const T dmp = (T)damping, added = (T)((1.0 - damping) * (1.0 / (double)n));
+  // FP32: the contributions of the highest out-degree sources come from each
+  // SM's shared memory (hub_cache tunable; same values, same sums)
+  HubCache<T> hubs;
+  if constexpr (std::is_same<T, float>::value) {
+    ensure_hubs(g);
+    if (g->hub_count > 0) hubs = HubCache<T>{g->hub_idx.as<int32_t>(), g->hub_vals.as<T>(), g->hub_count};
+  }
   E.run_loop(loop_key("pagerank", (int)sizeof(T), iters, damping, pc, pn, c0, c1, d_resid), [&] {
     T *a = pc, *b = pn, *x = c0, *y = c1;
     for (int it = 0; it < iters; ++it) {
       PM_CUDA(cudaMemsetAsync(E.d_cnt, 0, sizeof(Counters), E.stream));
       E.prof.begin("pagerank", E.stream);
-      launch_pull_reduce<int>(E, PR_F<T>{x, y, a, b, deg_off, dmp, added}, nullptr, nullptr, E.d_cnt);
+      if constexpr (std::is_same<T, float>::value)
+        if (hubs.count > 0) hub_values(g, x);
+      launch_pull_reduce<int>(E, PR_F<T>{x, y, a, b, deg_off, dmp, added}, nullptr, nullptr, E.d_cnt, hubs);
       E.prof.end(E.stream);
       part_exchange(g, y, sizeof(T));  // a partition: next contributions of every rank
       if (d_resid) PM_LAUNCH(k_copy_daux, 1, 1, 0, E.stream, E.d_cnt, d_resid + it);

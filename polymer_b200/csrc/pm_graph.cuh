@@ -133,6 +133,12 @@ struct pm_graph : pm::IdleFreeBase {
   int64_t part_lo = 0, part_hi = 0;
   std::vector<int64_t> part_bounds, part_wbounds;
   pm::DevBuf glob_off;
+  // hub cache of the FP32 PageRank pull (pm_hubs.cu): the hub_count sources
+  // of highest out-degree (hub_ids), the CSC sources with theirs tagged as
+  // ~slot (hub_idx) and a pass's copy of their values (hub_vals); built for
+  // hub_for sources at most (-1: not built)
+  pm::DevBuf hub_ids, hub_idx, hub_vals;
+  int hub_count = 0, hub_for = -1;
   int (*part_fn)(void *user, void *buf, int64_t elem_bytes, const int64_t *bounds, int nranks,
                  void *stream) = nullptr;
   void *part_user = nullptr;
@@ -166,6 +172,11 @@ void permute_weights_f32(pm_graph *g);
 // The float weights paired with their CSC source ids, or with their CSR
 // destination ids when csr (built once per weights).
 const WPair *ensure_f32_pairs(pm_graph *g, bool csr = false);
+
+// Hub tables for the handle's hub_cache tunable (rebuilt when it changed).
+void ensure_hubs(pm_graph *g);
+// vals[i] = x[ids[i]]: the cached sources' values for one pass.
+void hub_values(pm_graph *g, const float *x);
 
 // ---- 1D vertex partition (pm_partition.cu) ----
 // Splits the validated CSR's vertices into nranks ranges of about equal

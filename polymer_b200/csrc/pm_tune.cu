@@ -39,6 +39,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_BF_DIV: return t.bf_div;
     case PM_TUNE_CUDA_GRAPHS: return t.cuda_graphs;
     case PM_TUNE_HEAVY_MODE: return t.heavy_mode;
+    case PM_TUNE_HUB_CACHE: return t.hub_cache;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -85,6 +86,9 @@ void check_tunable(int key, int64_t value) {
       break;
     case PM_TUNE_HEAVY_MODE:
       if (value < 0 || value > 2) fail(PM_ERR_INVALID_ARG, "heavy_mode must be 0, 1 or 2");
+      break;
+    case PM_TUNE_HUB_CACHE:
+      if (value < 0 || value > kHubMax) fail(PM_ERR_INVALID_ARG, "hub_cache must be in [0, 16384]");
       break;
     default:
       fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));

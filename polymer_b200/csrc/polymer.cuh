@@ -466,6 +466,42 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
 #endif
 constexpr int kLaneEdges = PM_LANE_EDGES;
 constexpr int kPullBlock = PM_PULL_BLOCK;
+// The pull with a hub cache runs two CTAs of kHubBlock threads per SM (the
+// 48 warps of the plain pull at its occupancy limit, 40 registers each), so
+// each SM holds two copies of the cached values, kHubMax of them at most
+// (64 KB each in FP32).
+constexpr int kHubBlock = 768;
+constexpr int kHubMax = 16384;
+
+// Sources whose values a pull keeps in shared memory: idx is the CSC source
+// array with the cached sources' slots stored as ~slot, vals their values
+// for this pass.
+template <class V>
+struct HubCache {
+  const int32_t *idx = nullptr;
+  const V *vals = nullptr;
+  int count = 0;
+};
+
+// Functors that can take a cached value declare kHubs and edge_value(v, row,
+// w) = edge(s, row, w) for v the value edge() would load for s.
+template <class F, class = void>
+struct HubTrait {
+  static constexpr bool value = false;
+};
+template <class F>
+struct HubTrait<F, std::void_t<decltype(F::kHubs)>> {
+  static constexpr bool value = F::kHubs;
+};
+
+template <bool HUBS, class F, class WV>
+__device__ __forceinline__ typename F::Acc pull_edge(const F &f, int s, int row, WV wv,
+                                                     const typename F::Acc *s_hub) {
+  if constexpr (HUBS) {
+    if (s < 0) return f.edge_value(s_hub[~s], row, wv);
+  }
+  return f.edge(s, row, wv);
+}
 template <class F, class W>
 __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f,
                                                                 const W *__restrict__ w,
@@ -559,15 +595,28 @@ constexpr int kHeavyWaitSpins = 1 << 22;  // x ~256 ns: gives up after about a s
 // every group ticket, so its warp is already running.  MODE 2 (overlapped):
 // k_heavy_reduce runs at the same time on a second stream and this kernel
 // leaves the heavy rows alone; k_heavy_commit commits them afterwards.
-template <class F, class W, int MODE = 0>
-__global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphView g, F f, const W *__restrict__ w,
-                                                     typename F::Acc *partials, int32_t *hdone,
-                                                     uint32_t *__restrict__ next, Counters *cnt) {
+//
+// HUBS (MODE 0 only): the light rows' sources come from hubs.idx, where the
+// cached sources appear as ~slot and their values are read from shared
+// memory (loaded from hubs.vals once per CTA); two kHubBlock-thread CTAs per
+// SM.  The values are the ones edge() would load, so results are unchanged.
+template <class F, class W, int MODE = 0, bool HUBS = false>
+__global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_PULL_MINB)
+    k_pull_reduce(GraphView g, F f, const W *__restrict__ w, typename F::Acc *partials, int32_t *hdone,
+                  uint32_t *__restrict__ next, Counters *cnt, HubCache<typename F::Acc> hubs = {}) {
   using Acc = typename F::Acc;
-  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges, NW = kPullBlock / 32;
+  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges, NW = (HUBS ? kHubBlock : kPullBlock) / 32;
   __shared__ Acc s_acc[NW][32];
   __shared__ int s_pos[NW][33];
   __shared__ int s_off[NW][32];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  Acc *s_hub = reinterpret_cast<Acc *>(s_dyn);
+  const int32_t *lidx = g.in.idx;  // light rows' sources
+  if constexpr (HUBS) {
+    for (int i = threadIdx.x; i < hubs.count; i += kHubBlock) s_hub[i] = hubs.vals[i];
+    __syncthreads();
+    lidx = hubs.idx;
+  }
   const int lane = lane_id(), wid = threadIdx.x >> 5;
   Acc *acc_s = s_acc[wid];
   int *pos_s = s_pos[wid];
@@ -633,11 +682,12 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
         typename EdgeT<W>::type wv[K];
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          src[k] = (32 * k + lane < cnt) ? load_src(g.in.idx, w, (int64_t)e0 + 32 * k + lane, wv[k]) : 0;
+          src[k] = (32 * k + lane < cnt) ? load_src(lidx, w, (int64_t)e0 + 32 * k + lane, wv[k]) : 0;
 #pragma unroll
         for (int k = 0; k < K; ++k)
           if (32 * k + lane < cnt)
-            s = f.combine(s, f.edge(src[k], rb + j0, edge_w(w, (int64_t)e0 + 32 * k + lane, wv[k])));
+            s = f.combine(s, pull_edge<HUBS>(f, src[k], rb + j0, edge_w(w, (int64_t)e0 + 32 * k + lane, wv[k]),
+                                             s_hub));
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) s = f.combine(s, shfl_down(s, d));
         if (lane == 0) acc_s[j0] = f.combine(acc_s[j0], s);
@@ -663,11 +713,12 @@ __global__ void __launch_bounds__(kPullBlock, PM_PULL_MINB) k_pull_reduce(GraphV
       }
       typename EdgeT<W>::type wv[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? load_src(g.in.idx, w, es[k], wv[k]) : 0;
+      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? load_src(lidx, w, es[k], wv[k]) : 0;
       Acc vals[K];
 #pragma unroll
       for (int k = 0; k < K; ++k)
-        vals[k] = (q0 + k < total) ? f.edge(src[k], rb + rows[k], edge_w(w, es[k], wv[k])) : f.identity();
+        vals[k] = (q0 + k < total) ? pull_edge<HUBS>(f, src[k], rb + rows[k], edge_w(w, es[k], wv[k]), s_hub)
+                                   : f.identity();
       // Local fold: the first segment is the head, rows that start and end
       // inside the lane are stored directly, the last segment is the tail.
       Acc head = f.identity(), run = f.identity();
@@ -1050,6 +1101,7 @@ struct Tunables {
   int32_t cuda_graphs = 1;           // capture the fixed-iteration loops
   int32_t heavy_mode = 0;            // heavy chunks: 0 a launch before the pull, 1 inside it,
                                      // 2 a launch beside it on a second stream
+  int32_t hub_cache = 0;             // FP32 PageRank: sources cached in shared memory (0 = off)
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
@@ -1271,11 +1323,32 @@ void launch_dense_push(Engine &E, VertexSubset &cur, F f, const W *w_out, Vertex
 // Pull-reduce over the CSC into counters cnt (size / edges of the output,
 // daux = sum of the FP64 values commit() adds); next_bits may be null.
 template <class W, class F>
-void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Counters *cnt) {
+void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Counters *cnt,
+                        HubCache<typename F::Acc> hubs = {}) {
   static_assert(sizeof(typename F::Acc) <= 16, "accumulator larger than the partials slot");
   using Acc = typename F::Acc;
   Acc *partials = reinterpret_cast<Acc *>(E.partials);
   const int mode = E.g.in.nchunks > 0 ? E.tune.heavy_mode : 0;
+  if constexpr (HubTrait<F>::value) {
+    if (hubs.count > 0 && mode == 0) {
+      // kHubBlock-thread CTAs, each holding the cached values
+      static const int hub_per_sm = [] {
+        PM_CUDA(cudaFuncSetAttribute((const void *)k_pull_reduce<F, W, 0, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, kHubMax * (int)sizeof(Acc)));
+        int r = 0;
+        PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_pull_reduce<F, W, 0, true>, kHubBlock,
+                                                              kHubMax * sizeof(Acc)));
+        return std::max(r, 1);
+      }();
+      if (E.g.in.nchunks > 0)
+        PM_LAUNCH((k_heavy_reduce<F, W>), E.g.in.nchunks, kChunkThreads, 0, E.stream, E.g, f, w_in, partials);
+      const int64_t want = ((int64_t)E.g.in.ngroups + kHubBlock / 32 - 1) / (kHubBlock / 32);
+      PM_LAUNCH((k_pull_reduce<F, W, 0, true>), E.persistent_grid(want, hub_per_sm), kHubBlock,
+                (size_t)hubs.count * sizeof(Acc), E.stream, E.g, f, w_in, partials, (int32_t *)nullptr, next_bits,
+                cnt, hubs);
+      return;
+    }
+  }
   if (mode == 1) {
     PM_CUDA(cudaMemsetAsync(E.hdone, 0, (size_t)E.g.in.nchunks * 4, E.stream));
   } else if (mode == 2) {
