@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-tune", action="store_true",
                    help="keep the default tunables instead of running the autotuner at setup")
+    p.add_argument("--no-cuda-graphs", action="store_true",
+                   help="launch every kernel directly (the same work): for profilers that cannot see "
+                        "kernels inside CUDA graphs with conditional nodes (the device-driven BFS rounds)")
     return p.parse_args()
 
 
@@ -792,6 +795,9 @@ def main():
     suite = Suite(pm, local, args.scale_a, args.scale_b, args.sources, rank)
     if not args.no_tune:
         suite.tune()
+    if args.no_cuda_graphs:
+        for g in (suite.A, suite.B):
+            g.set_tunable("cuda_graphs", 0)
     per = {}
     for _ in range(args.warmup):
         suite.step({})
@@ -848,6 +854,8 @@ def main():
             "l2": "inputs larger than L2 (126 MB): graph A ids %d MB, graph B ids %d MB"
                   % (suite.A.m * 4 >> 20, mB * 4 >> 20),
             "parallelism": "replicas x%d" % world,
+            "launch": "direct launches (--no-cuda-graphs)" if args.no_cuda_graphs else
+                      "CUDA graphs: captured PageRank/SpMV/BP loops, device-driven BFS rounds",
         },
         "per_algo": per_algo,
         "roofline": {
