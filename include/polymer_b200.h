@@ -415,7 +415,9 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       SpMV, BP and PPR run as CUDA graphs, captured the
                                       second time a handle runs the same loop (same
                                       sizes, buffers and scalars) and replayed from
-                                      then on; 0: plain launches */
+                                      then on, and BFS runs its rounds inside one CUDA
+                                      graph whose WHILE node chooses each round's
+                                      direction on the GPU; 0: plain launches */
 #define PM_TUNE_HEAVY_MODE 8       /* how the chunks of heavy rows are summed: 0 (default)
                                       a launch before the pull; 1 inside the pull launch
                                       (warps take them first, a row's lane waits for its
