@@ -154,7 +154,8 @@ PMO_API int64_t pmo_er_batch(int count, int64_t n_min, int64_t n_max, int avg_de
   return m;
 }
 
-/* Edge weight rules shared with the GPU generator (see DESIGN data layout). */
+/* Edge weight rules shared with the GPU generator (k_weights_i32 / k_weights_f32):
+ * a hash of the edge's endpoints, so both sides draw the same weight per edge. */
 PMO_API int32_t pmo_weight_int(uint64_t seed, uint32_t u, uint32_t v, int32_t wmax) {
   uint32_t a = u < v ? u : v, b = u < v ? v : u; /* symmetric: w(u,v) == w(v,u) */
   uint64_t key = ((uint64_t)a << 32) | b;
