@@ -141,7 +141,10 @@ PM_API pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count
  * pm_spmv, pm_bfs, pm_components and pm_bellman_ford run on a partition and
  * return the whole result on every rank (the optional residual / norm
  * arrays and the statistics count this rank's rows and edges); the other
- * application calls return PM_ERR_NOT_SUPPORTED.  nranks 1..1024. */
+ * application calls return PM_ERR_NOT_SUPPORTED.  On a partition handle,
+ * pm_graph_info gives the whole graph's n and this rank's edge count, and
+ * pm_graph_get_csr this rank's edges (all n sources, global ids).
+ * nranks 1..1024. */
 typedef int (*pm_allgather_fn)(void *user, void *buf, int64_t elem_bytes, const int64_t *bounds, int nranks,
                                void *stream);
 PM_API pm_status pm_graph_create_partition(const int32_t *offsets, const int32_t *edges, const void *weights,
