@@ -406,9 +406,10 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
 #define PM_TUNE_HEAVY_DEG 0        /* rows with more edges are split in 4096-edge chunks
                                       (default 2048, range [64, 2^30]) */
 #define PM_TUNE_CTA_EXPAND 1       /* sparse push: CTA-wide expansion from this
-                                      out-degree (default 512) */
+                                      out-degree (default 128) */
 #define PM_TUNE_GRID_EXPAND 2      /* sparse push: grid-wide expansion from this
-                                      out-degree (default 4096) */
+                                      out-degree (default 256; at most 4096 such rows per
+                                      round, the rest expand CTA-wide) */
 #define PM_TUNE_PULL_CTAS_PER_SM 3 /* resident CTAs per SM of the persistent pulls,
                                       0 = the occupancy limit (default) */
 #define PM_TUNE_BFS_DIV 4          /* threshold < 0 means m / div: BFS (default 20) */

@@ -235,8 +235,8 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
       std::vector<int64_t> cands;
       switch (key) {
         case PM_TUNE_HEAVY_DEG: cands = {512, 1024, 2048, 4096, 8192, 32768}; break;
-        case PM_TUNE_CTA_EXPAND: cands = {128, 256, 512, 1024, 2048}; break;
-        case PM_TUNE_GRID_EXPAND: cands = {2048, 4096, 16384, 65536}; break;
+        case PM_TUNE_CTA_EXPAND: cands = {64, 128, 256, 512}; break;
+        case PM_TUNE_GRID_EXPAND: cands = {128, 256, 512, 1024, 4096}; break;
         case PM_TUNE_HEAVY_MODE: cands = {0, 1, 2}; break;
         case PM_TUNE_PULL_CTAS_PER_SM:
           cands.push_back(0);
