@@ -221,7 +221,8 @@ PM_API pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32
  * sources[l], -1 when unreached) -- each row equals pm_bfs's depth for that
  * source.  sources: k int32 in mem's space.  stats->reached = sum over
  * sources of reached vertices; stats->edges_visited = sum over sources of the
- * out-degrees of the reached vertices. */
+ * out-degrees of the reached vertices.  threshold < 0: m / PM_TUNE_MSBFS_DIV
+ * (the union frontier of many sources turns dense sooner than one BFS's). */
 PM_API pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *depth,
                               uint32_t mem, int64_t threshold, pm_traversal_stats *stats);
 
@@ -432,6 +433,8 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       shared memory during a pass (0 = off, the default; at
                                       most 16384; results are unchanged; slower than the
                                       plain pull on the R-MAT workloads measured) */
+#define PM_TUNE_MSBFS_DIV 10       /* threshold < 0 means m / div: multi-source BFS
+                                      (default 8) */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */
