@@ -221,7 +221,7 @@ PM_API pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32
  * sources[l], -1 when unreached) -- each row equals pm_bfs's depth for that
  * source.  sources: k int32 in mem's space.  stats->reached = sum over
  * sources of reached vertices; stats->edges_visited = sum over sources of the
- * out-degrees of the reached vertices.  threshold < 0: m / PM_TUNE_MSBFS_DIV
+ * out-degrees of the reached vertices.  threshold < 0: m / PM_TUNE_MULTI_DIV
  * (the union frontier of many sources turns dense sooner than one BFS's). */
 PM_API pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *depth,
                               uint32_t mem, int64_t threshold, pm_traversal_stats *stats);
@@ -247,7 +247,7 @@ PM_API pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32
  * distance lanes per vertex (BF_F of numa-BellmanFord.C:61-85 per lane; the
  * reference runs one source per process).  The frontier is the set of
  * vertices with a lane that fell in the last round; the direction rule of
- * pm_bellman_ford applies to it (threshold < 0: m / PM_TUNE_BF_DIV).  dist: k*n
+ * pm_bellman_ford applies to it (threshold < 0: m / PM_TUNE_MULTI_DIV).  dist: k*n
  * int32, source-major (dist[l*n + v] = distance of v from sources[l],
  * 1073741823 when unreached) -- each row equals pm_bellman_ford's dist for
  * that source.  sources: k int32 in mem's space.  stats->reached = number of
@@ -433,8 +433,9 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       shared memory during a pass (0 = off, the default; at
                                       most 16384; results are unchanged; slower than the
                                       plain pull on the R-MAT workloads measured) */
-#define PM_TUNE_MSBFS_DIV 10       /* threshold < 0 means m / div: multi-source BFS
-                                      (default 8) */
+#define PM_TUNE_MULTI_DIV 10       /* threshold < 0 means m / div: multi-source BFS and
+                                      BellmanFord (default 8; their union frontiers turn
+                                      dense sooner than one source's) */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

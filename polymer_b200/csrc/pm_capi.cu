@@ -578,7 +578,7 @@ pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dept
     const int32_t *ds = stage_sources(g, sources, k, mem);
     const size_t bytes = (size_t)g->n * k * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? depth : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_msbfs(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.msbfs_div : threshold, stats);
+    run_msbfs(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.multi_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, depth, dd, bytes, mem);
     finish(g);
   });
@@ -595,7 +595,7 @@ pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int3
     const int32_t *ds = stage_sources(g, sources, k, mem);
     const size_t bytes = (size_t)g->n * k * 4;
     int32_t *dd = mem == PM_MEM_DEVICE ? dist : (int32_t *)g->scratch_buf(kSlotOut0, bytes);
-    run_bf_multi(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.bf_div : threshold, stats);
+    run_bf_multi(g, ds, k, dd, threshold < 0 ? g->m / g->E.tune.multi_div : threshold, stats);
     if (mem == PM_MEM_HOST) from_device(g, dist, dd, bytes, mem);
     finish(g);
   });

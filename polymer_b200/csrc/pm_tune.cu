@@ -40,7 +40,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_CUDA_GRAPHS: return t.cuda_graphs;
     case PM_TUNE_HEAVY_MODE: return t.heavy_mode;
     case PM_TUNE_HUB_CACHE: return t.hub_cache;
-    case PM_TUNE_MSBFS_DIV: return t.msbfs_div;
+    case PM_TUNE_MULTI_DIV: return t.multi_div;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -80,7 +80,7 @@ void check_tunable(int key, int64_t value) {
     case PM_TUNE_BFS_DIV:
     case PM_TUNE_CC_DIV:
     case PM_TUNE_BF_DIV:
-    case PM_TUNE_MSBFS_DIV:
+    case PM_TUNE_MULTI_DIV:
       if (value < 1 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "threshold divisor must be in [1, 2^30]");
       break;
     case PM_TUNE_CUDA_GRAPHS:

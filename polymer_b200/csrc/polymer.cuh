@@ -1107,7 +1107,7 @@ struct Tunables {
   int32_t heavy_mode = 0;            // heavy chunks: 0 a launch before the pull, 1 inside it,
                                      // 2 a launch beside it on a second stream
   int32_t hub_cache = 0;             // FP32 PageRank: sources cached in shared memory (0 = off)
-  int32_t msbfs_div = 8;             // multi-source BFS: default threshold = m / div
+  int32_t multi_div = 8;             // multi-source BFS / BellmanFord: default threshold = m / div
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
