@@ -50,3 +50,12 @@ def test_async_bfs_isolated_source_and_hub(pm, oracle):
         reached = check_tree(oracle, og, 0, par)
         assert reached.sum() == 10002 and st["reached"] == 10002
         assert np.all(par[1:10001] == 0) and 1 <= par[10001] <= 10000
+
+
+def test_async_bfs_long_chain(pm, oracle):
+    # one item in flight at a time: every warp's batch of slots waits for the chain
+    n = 2000
+    og = oracle.graph_from_edges(n, np.arange(n - 1), np.arange(1, n))
+    with pm.Graph.from_csr(og.off, og.idx) as g:
+        par, st = pm.BFSAsync(0, g, stats=True)
+        assert st["reached"] == n and par[0] == 0 and np.array_equal(par[1:], np.arange(n - 1))
