@@ -145,6 +145,8 @@ static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t 
     fresh.key = key;
     cudaGraph_t graph = nullptr;
     PM_CUDA(cudaGraphCreate(&graph, 0));
+    bool capturing = false;
+    const long long before = launches(false);
     try {
       cudaGraphConditionalHandle loop;
       PM_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
@@ -156,8 +158,8 @@ static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t 
       cudaGraphNode_t node;
       PM_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
       cudaGraph_t body = cp.conditional.phGraph_out[0];
-      const long long before = launches(false);
       PM_CUDA(cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      capturing = true;
       const int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
       const int qgrid = E.grid_for(((A.words() + 31) / 32) * 32, 256, 8);
       const int32_t max_level = (int32_t)std::min<int64_t>(g->n + 1, 0x7ffffff0);
@@ -181,10 +183,17 @@ static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t 
       round(A, B);
       round(B, A);
       cudaGraph_t captured = nullptr;
+      capturing = false;
       PM_CUDA(cudaStreamEndCapture(E.stream, &captured));
       count_launch((int)-(launches(false) - before));  // captured, not run
       PM_CUDA(cudaGraphInstantiate(&fresh.exec, graph, 0));
     } catch (...) {
+      if (capturing) {  // leave the stream usable; the body graph belongs to `graph`
+        cudaGraph_t captured = nullptr;
+        cudaStreamEndCapture(E.stream, &captured);
+        (void)cudaGetLastError();
+        count_launch((int)-(launches(false) - before));
+      }
       cudaGraphDestroy(graph);
       throw;
     }
