@@ -405,7 +405,7 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
  * CC m/8, numa-Components.C:226; BellmanFord m/20, numa-BellmanFord.C:182).
  * Results never depend on them; only speed does. */
 #define PM_TUNE_HEAVY_DEG 0        /* rows with more edges are split in 4096-edge chunks
-                                      (default 2048, range [64, 2^30]) */
+                                      (default 1024, range [64, 2^30]) */
 #define PM_TUNE_CTA_EXPAND 1       /* sparse push: CTA-wide expansion from this
                                       out-degree (default 128) */
 #define PM_TUNE_GRID_EXPAND 2      /* sparse push: grid-wide expansion from this

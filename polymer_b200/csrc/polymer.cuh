@@ -41,7 +41,7 @@ namespace pm {
 
 constexpr int kGroupWork = 1024;   // work units (edges + kRowWork per row) of one warp group
 constexpr int kRowWork = 4;       // a row costs about as much as this many edges
-constexpr int kHeavyDeg = 2048;    // default: rows above this degree are split in chunks
+constexpr int kHeavyDeg = 1024;    // default: rows above this degree are split in chunks
 constexpr int kChunkEdges = 4096;  // edges of one heavy chunk (one CTA)
 constexpr int kChunkThreads = 256;
 constexpr int kPullScan = 32;      // edges a thread scans before deferring a row

@@ -60,7 +60,7 @@ def test_default_tunables_host_only():
     """The process-wide tunables (NULL handle) are host state: set, read back,
     range-checked and restored without a GPU."""
     import polymer_b200 as pm
-    defaults = {"heavy_deg": 2048, "cta_expand": 128, "grid_expand": 256, "pull_ctas_per_sm": 0,
+    defaults = {"heavy_deg": 1024, "cta_expand": 128, "grid_expand": 256, "pull_ctas_per_sm": 0,
                 "bfs_div": 20, "cc_div": 8, "bf_div": 20, "cuda_graphs": 1, "multi_div": 8}
     assert {k: pm.get_default_tunable(k) for k in defaults} == defaults
     try:

@@ -167,10 +167,10 @@ def test_defaults_apply_to_new_graphs(pm, oracle):
             assert g.get_tunable("heavy_deg") == 256 and g.get_tunable("cuda_graphs") == 0
             assert rel_l1(pm.PageRank(g, 10, dtype=np.float32), ref) < RL1_F32
     finally:
-        pm.set_default_tunable("heavy_deg", 2048)
+        pm.set_default_tunable("heavy_deg", 1024)
         pm.set_default_tunable("cuda_graphs", 1)
     with pm.Graph.from_csr(og.off, og.idx) as g:
-        assert g.get_tunable("heavy_deg") == 2048
+        assert g.get_tunable("heavy_deg") == 1024
 
 
 def test_autotuner_mix_keeps_results(pm, oracle):
