@@ -120,19 +120,15 @@ __global__ void k_round_end(DevRound *dr, const Counters *cnt, cudaGraphConditio
   cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
-constexpr int kRoundKernels = 7;  // kernels of one round in the loop body
-
-static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
-                          pm_traversal_stats *st) {
+// Runs a traversal's rounds inside one CUDA graph (built once per key): a
+// WHILE node whose body is round(A, B) then round(B, A), each between
+// k_round_begin and k_round_end.  The round state in dr is set up on the
+// stream before the call; on return it is read back into h.
+template <class Round>
+static void run_rounds(pm_graph *g, DevRound *dr, const std::string &key, int64_t threshold, const char *tag,
+                       Round &&round, DevRound &h) {
   Engine &E = g->E;
   VertexSubset A = g->subset(0), B = g->subset(1);
-  auto *dr = (DevRound *)g->scratch_buf(30, sizeof(DevRound));
-  PM_LAUNCH(k_bfs_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_parents, d_depth, g->n, src);
-  PM_CUDA(cudaMemsetAsync(A.bits, 0, A.words() * 4, E.stream));
-  PM_LAUNCH(k_round_init, 1, 1, 0, E.stream, dr, A.bits, E.g.out.off, src);
-  char key[160];
-  std::snprintf(key, sizeof key, "bfs_rounds|%lld|%p|%p|%p", (long long)threshold, (void *)d_parents,
-                (void *)d_depth, (void *)dr);
   LoopGraph *lg = nullptr;
   for (auto &x : E.graphs)
     if (x.key == key) lg = &x;
@@ -160,32 +156,20 @@ static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t 
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       PM_CUDA(cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
       capturing = true;
-      const int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
-      const int qgrid = E.grid_for(((A.words() + 31) / 32) * 32, 256, 8);
       const int32_t max_level = (int32_t)std::min<int64_t>(g->n + 1, 0x7ffffff0);
-      auto round = [&](VertexSubset &cur, VertexSubset &next) {
-        const BFS_GF f{d_parents, d_depth, &dr->gate};
-        const RoundGate *gate = &dr->gate;
+      auto one = [&](VertexSubset &cur, VertexSubset &next) {
         PM_LAUNCH(k_round_begin, 1, 1, 0, E.stream, dr, E.d_cnt, threshold);
-        PM_CUDA(cudaMemsetAsync(next.bits, 0, next.words() * 4, E.stream));
-        PM_LAUNCH(k_bits_to_queue, qgrid, 256, 0, E.stream, cur.n, E.g.out.off, cur.bits, cur.queue, E.d_cnt + 2,
-                  gate);
-        PM_LAUNCH((k_sparse_push<BFS_GF, int>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.queue, 0, f,
-                  (const int *)nullptr, next.queue, next.bits, next.n, E.d_cnt, E.hubs, E.d_cnt + 1, gate);
-        PM_LAUNCH((k_sparse_push_hubs<BFS_GF, int>), E.num_sms * 4, 256, 0, E.stream, E.g, f, (const int *)nullptr,
-                  E.hubs, E.d_cnt + 1, next.queue, next.bits, next.n, E.d_cnt, gate);
-        PM_LAUNCH((k_dense_pull<BFS_GF, int>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, E.g, cur.bits, f,
-                  (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
-        PM_LAUNCH((k_dense_pull_defer<BFS_GF, int>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.bits, f,
-                  (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
+        round(cur, next, (const RoundGate *)&dr->gate);
         PM_LAUNCH(k_round_end, 1, 1, 0, E.stream, dr, E.d_cnt, loop, max_level);
       };
-      round(A, B);
-      round(B, A);
+      one(A, B);
+      one(B, A);
       cudaGraph_t captured = nullptr;
       capturing = false;
       PM_CUDA(cudaStreamEndCapture(E.stream, &captured));
-      count_launch((int)-(launches(false) - before));  // captured, not run
+      const long long captured_launches = launches(false) - before;
+      fresh.launches = captured_launches / 2;  // kernels of one round
+      count_launch((int)-captured_launches);   // captured, not run
       PM_CUDA(cudaGraphInstantiate(&fresh.exec, graph, 0));
     } catch (...) {
       if (capturing) {  // leave the stream usable; the body graph belongs to `graph`
@@ -201,25 +185,64 @@ static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t 
     E.graphs.push_back(std::move(fresh));
     lg = &E.graphs.back();
   }
-  E.prof.begin("bfs", E.stream);
+  E.prof.begin(tag, E.stream);
   PM_CUDA(cudaGraphLaunch(lg->exec, E.stream));
   E.prof.end(E.stream);
-  DevRound h{};
   PM_CUDA(cudaMemcpyAsync(E.h_cnt, dr, sizeof(DevRound), cudaMemcpyDeviceToHost, E.stream));
   PM_CUDA(cudaStreamSynchronize(E.stream));
   std::memcpy(&h, E.h_cnt, sizeof h);
-  count_launch((int)(kRoundKernels * h.slots));
+  count_launch((int)(lg->launches * (long long)h.slots));
   if (h.err)
     fail(h.err & kErrTimeout ? PM_ERR_TIMEOUT : PM_ERR_CUDA,
          std::string("device error word ") + std::to_string(h.err) +
              (h.err & kErrQueueOverflow ? " (queue overflow)" : "") + (h.err & kErrRange ? " (id out of range)" : ""));
-  if (st) {
-    *st = pm_traversal_stats{};
-    st->rounds = (int64_t)h.rounds;
-    st->dense_rounds = (int64_t)h.dense_rounds;
-    st->reached = (int64_t)h.reached;
-    st->edges_visited = (int64_t)h.edges_visited;
-  }
+}
+
+// The sparse half of a round driven on the GPU (returns at once in dense
+// rounds): the frontier bitmap to a queue, then the push.
+template <class F, class W>
+static void gated_sparse(Engine &E, VertexSubset &cur, VertexSubset &next, F f, const W *w_out,
+                         const RoundGate *gate) {
+  PM_CUDA(cudaMemsetAsync(next.bits, 0, next.words() * 4, E.stream));
+  PM_LAUNCH(k_bits_to_queue, E.grid_for(((cur.words() + 31) / 32) * 32, 256, 8), 256, 0, E.stream, cur.n,
+            E.g.out.off, cur.bits, cur.queue, E.d_cnt + 2, gate);
+  PM_LAUNCH((k_sparse_push<F, W>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.queue, 0, f, w_out, next.queue,
+            next.bits, next.n, E.d_cnt, E.hubs, E.d_cnt + 1, gate);
+  PM_LAUNCH((k_sparse_push_hubs<F, W>), E.num_sms * 4, 256, 0, E.stream, E.g, f, w_out, E.hubs, E.d_cnt + 1,
+            next.queue, next.bits, next.n, E.d_cnt, gate);
+}
+
+static void fill_stats(const DevRound &h, pm_traversal_stats *st) {
+  if (!st) return;
+  *st = pm_traversal_stats{};
+  st->rounds = (int64_t)h.rounds;
+  st->dense_rounds = (int64_t)h.dense_rounds;
+  st->reached = (int64_t)h.reached;
+  st->edges_visited = (int64_t)h.edges_visited;
+}
+
+static void run_bfs_graph(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,
+                          pm_traversal_stats *st) {
+  Engine &E = g->E;
+  VertexSubset A = g->subset(0);
+  auto *dr = (DevRound *)g->scratch_buf(30, sizeof(DevRound));
+  PM_LAUNCH(k_bfs_init, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_parents, d_depth, g->n, src);
+  PM_CUDA(cudaMemsetAsync(A.bits, 0, A.words() * 4, E.stream));
+  PM_LAUNCH(k_round_init, 1, 1, 0, E.stream, dr, A.bits, E.g.out.off, src);
+  char key[160];
+  std::snprintf(key, sizeof key, "bfs_rounds|%lld|%p|%p|%p", (long long)threshold, (void *)d_parents,
+                (void *)d_depth, (void *)dr);
+  const int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
+  DevRound h{};
+  run_rounds(g, dr, key, threshold, "bfs", [&](VertexSubset &cur, VertexSubset &next, const RoundGate *gate) {
+    const BFS_GF f{d_parents, d_depth, gate};
+    gated_sparse<BFS_GF, int>(E, cur, next, f, (const int *)nullptr, gate);
+    PM_LAUNCH((k_dense_pull<BFS_GF, int>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, E.g, cur.bits, f,
+              (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
+    PM_LAUNCH((k_dense_pull_defer<BFS_GF, int>), E.num_sms * 8, 256, 0, E.stream, E.g, cur.bits, f,
+              (const int *)nullptr, next.bits, E.defer, E.d_cnt, E.d_cnt + 1, gate);
+  }, h);
+  fill_stats(h, st);
 }
 
 void run_bfs(pm_graph *g, int32_t src, int32_t *d_parents, int32_t *d_depth, int64_t threshold,

@@ -66,3 +66,4 @@ def test_replays_with_other_sources(pm, oracle):
         srcs = [int(s) for s in oracle.pick_sources(og, 6)]
         for s in srcs + srcs[::-1]:
             assert np.array_equal(pm.BFS(s, g)[1], oracle.bfs(og, s)[0])
+
