@@ -501,6 +501,7 @@ struct SPMV_F {
   const T *x;
   T *y;
   using Acc = T;
+  static constexpr int kLaneEdges = 5;  // 5 % faster per pass than 6 at scale 24
   __device__ __forceinline__ bool cond(int) const { return true; }
   __device__ __forceinline__ Acc identity() const { return T(-0.0); }
   __device__ __forceinline__ Acc edge(int s, int, float w) const { return T(w) * __ldg(x + s); }
@@ -563,6 +564,7 @@ struct BP_F {
   const V *prior;
   T p00, p01, p10, p11;
   using Acc = int32_t;
+  static constexpr int kLaneEdges = 5;  // 2 % faster per pass than 6 at scale 24
   __device__ __forceinline__ bool cond(int) const { return true; }
   __device__ __forceinline__ Acc identity() const { return 0; }
   __device__ __forceinline__ Acc edge(int s, int, int) const { return test_bit(cur, s) ? 1 : 0; }

@@ -502,6 +502,17 @@ struct HubTrait<F, std::void_t<decltype(F::kHubs)>> {
   static constexpr bool value = F::kHubs;
 };
 
+// Edges per lane of a functor's light pull: F::kLaneEdges when it declares
+// one, else kLaneEdges (the best values differ by functor: measured per pass).
+template <class F, class = void>
+struct LaneEdgesTrait {
+  static constexpr int value = kLaneEdges;
+};
+template <class F>
+struct LaneEdgesTrait<F, std::void_t<decltype(F::kLaneEdges)>> {
+  static constexpr int value = F::kLaneEdges;
+};
+
 template <bool HUBS, class F, class WV>
 __device__ __forceinline__ typename F::Acc pull_edge(const F &f, int s, int row, WV wv,
                                                      const typename F::Acc *s_hub) {
@@ -613,7 +624,7 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
     k_pull_reduce(GraphView g, F f, const W *__restrict__ w, typename F::Acc *partials, int32_t *hdone,
                   uint32_t *__restrict__ next, Counters *cnt, HubCache<typename F::Acc> hubs = {}) {
   using Acc = typename F::Acc;
-  constexpr int K = kLaneEdges, WIN = 32 * kLaneEdges, NW = (HUBS ? kHubBlock : kPullBlock) / 32;
+  constexpr int K = LaneEdgesTrait<F>::value, WIN = 32 * K, NW = (HUBS ? kHubBlock : kPullBlock) / 32;
   __shared__ Acc s_acc[NW][32];
   __shared__ int s_pos[NW][33];
   __shared__ int s_off[NW][32];
