@@ -138,7 +138,7 @@ PM_API pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count
  *   the gathered buf (an NCCL allgather-v on that stream, for instance);
  *   return 0, or nonzero to fail the running call with PM_ERR_CUDA.
  * Every rank must run the same calls in the same order.  pm_pagerank,
- * pm_spmv, pm_bfs, pm_components and pm_bellman_ford run on a partition and
+ * pm_spmv, pm_bp, pm_bfs, pm_components and pm_bellman_ford run on a partition and
  * return the whole result on every rank (the optional residual / norm
  * arrays and the statistics count this rank's rows and edges); the other
  * application calls return PM_ERR_NOT_SUPPORTED.  On a partition handle,

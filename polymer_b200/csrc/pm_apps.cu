@@ -613,10 +613,12 @@ void run_bp(pm_graph *g, const T *d_prior, const T *psi, int iters, T *d_out) {
                      E, BP_F<T>{fa, a, b, (const V *)d_prior, psi[0], psi[1], psi[2], psi[3]}, nullptr,
                      fb, E.d_cnt);
                  E.prof.end(E.stream);
+                 part_exchange_bits(g, fb);  // a partition: the next frontier of every rank
                  std::swap(a, b);
                  std::swap(fa, fb);
                }
              });
+  part_exchange(g, iters % 2 ? ln : lc, sizeof(V));  // a partition: every rank's log-products
   PM_CUDA(cudaMemcpyAsync(d_out, iters % 2 ? ln : lc, (size_t)n * sizeof(V), cudaMemcpyDeviceToDevice,
                           E.stream));
 }

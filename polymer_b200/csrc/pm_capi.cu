@@ -139,7 +139,7 @@ static void from_device(pm_graph *g, void *dst, const void *src, size_t bytes, u
 }
 static void finish(pm_graph *g) { PM_CUDA(cudaStreamSynchronize(g->E.stream)); }
 static void check_mem(uint32_t mem) { need(mem == PM_MEM_HOST || mem == PM_MEM_DEVICE, "mem must be PM_MEM_HOST or PM_MEM_DEVICE"); }
-// The calls a partition graph serves: pm_pagerank, pm_spmv, pm_bfs,
+// The calls a partition graph serves: pm_pagerank, pm_spmv, pm_bp, pm_bfs,
 // pm_components, pm_bellman_ford (and the handle queries); the others need
 // the whole graph on one device.
 static void whole_graph(const pm_graph *g, const char *what) {
@@ -830,7 +830,6 @@ extern "C++" {
 template <class T>
 static void bp_call(pm_graph *g, const T *prior, const T *psi, int iters, T *log_prod, uint32_t mem) {
   enter(g);
-  whole_graph(g, "pm_bp");
   check_mem(mem);
   need(prior != nullptr && psi != nullptr && log_prod != nullptr, "null prior/psi/log_prod");
   need(iters >= 0, "iters must be >= 0");

@@ -188,6 +188,8 @@ void restrict_to_partition(pm_graph *g, int rank, int nranks, DevBuf *w);
 // Every rank's range of buf (n entries of elem_bytes) into every rank's
 // buf, through the handle's exchange function, in stream order.
 void part_exchange(pm_graph *g, void *buf, size_t elem_bytes);
+// Every rank's words of a frontier bitmap into every rank's copy.
+void part_exchange_bits(pm_graph *g, uint32_t *bits);
 // After a round on a partition: the next frontier's bitmap made global, its
 // size and out-degree sum recounted.
 void part_round(pm_graph *g, VertexSubset &next);

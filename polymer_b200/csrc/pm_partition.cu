@@ -152,6 +152,13 @@ void part_exchange(pm_graph *g, void *buf, size_t elem_bytes) {
   if (rc != 0) fail(PM_ERR_CUDA, "partition exchange function returned " + std::to_string(rc));
 }
 
+void part_exchange_bits(pm_graph *g, uint32_t *bits) {
+  if (!g->is_part || g->part_count == 1) return;
+  if (!g->part_fn) fail(PM_ERR_INVALID_ARG, "partition graph without an exchange function (pm_graph_set_exchange)");
+  const int rc = g->part_fn(g->part_user, bits, 4, g->part_wbounds.data(), g->part_count, (void *)g->E.stream);
+  if (rc != 0) fail(PM_ERR_CUDA, "partition exchange function returned " + std::to_string(rc));
+}
+
 void part_round(pm_graph *g, VertexSubset &next) {
   if (!g->is_part) return;
   if (g->part_count > 1) {

@@ -4,7 +4,7 @@ its vertex range, with the ranges exchanged after every pass.  The P ranks
 run as host threads on one GPU (partition_local.LocalGroup); every rank's
 result must be the whole graph's result, checked against the oracle:
 PageRank and SpMV (FP64) to 1e-10, BFS depths, Components labels and
-BellmanFord distances exactly."""
+BellmanFord distances exactly, BP bit for bit against the whole graph."""
 import numpy as np
 import pytest
 
@@ -34,6 +34,25 @@ def test_pagerank_spmv_directed(pm, oracle, nranks):
         assert k == nranks
         assert np.allclose(pr, want_pr, rtol=1e-10, atol=0)
         assert np.allclose(y, want_y, rtol=1e-10, atol=1e-300)
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_bp_bit_identical(pm, oracle, nranks):
+    """BP's pull sums integer counts of frontier in-neighbours, so a partition
+    gives the whole graph's log-products bit for bit (FP32 and FP64)."""
+    og = oracle.rmat_graph(13, 16)
+    prior = oracle.uniform_open(2 * og.n).reshape(-1, 2).astype(np.float32)
+    with pm.Graph.from_csr(og.off, og.idx) as g:
+        want32 = pm.BeliefPropagation(g, prior, 7)
+        want64 = pm.BeliefPropagation(g, prior.astype(np.float64), 7, dtype=np.float64)
+
+    def body(rank, ex):
+        with _part(pm, og, rank, nranks, ex) as g:
+            return (pm.BeliefPropagation(g, prior, 7),
+                    pm.BeliefPropagation(g, prior.astype(np.float64), 7, dtype=np.float64))
+
+    for b32, b64 in LocalGroup(nranks).run(body):
+        assert np.array_equal(b32, want32) and np.array_equal(b64, want64)
 
 
 @pytest.mark.parametrize("nranks", [2, 4])
@@ -107,9 +126,6 @@ def test_whole_graph_calls_refused_and_exchange_errors(pm, oracle):
         with _part(pm, og, rank, 2, ex) as g:
             with pytest.raises(pm.PolymerError) as ei:
                 pm.PersonalizedPageRank(g, [0], 2)
-            assert ei.value.status == 6
-            with pytest.raises(pm.PolymerError) as ei:
-                pm.BeliefPropagation(g, np.full((og.n, 2), 0.5, np.float32), 2)
             assert ei.value.status == 6
         return True
 
