@@ -4,7 +4,9 @@ polymer_b200.distributed.allgather_v (an empty range included), and run
 PageRank on a 1D partition -- each rank reduces only its own rows with the
 reference's frontier semantics (numa-PageRank.C PR_F / PR_Vertex_F /
 PR_Vertex_Reset) and the contributions and frontier are gathered after
-every pass -- which must equal the oracle's whole-graph PageRank.  The
+every pass -- which must equal the oracle's whole-graph PageRank, and
+Components by min-label propagation with labels and frontier gathered after
+every round -- the oracle's labels, both ranks ending in the same round.  The
 ranges come from partition_bounds, the host restatement of the library's
 cut rule.  No GPU is used."""
 import os
@@ -56,6 +58,34 @@ def _pagerank_partitioned(og, bounds, rank, ex, iters, damping=0.85):
     return pc
 
 
+def _components_partitioned(og, bounds, rank, ex):
+    """Min-label propagation (numa-Components.C CC_F) over this rank's rows:
+    labels and the frontier are gathered after every round; every rank sees
+    the same global frontier, so all stop in the same round."""
+    n = og.n
+    deg = np.diff(og.off).astype(np.int64)
+    src = np.repeat(np.arange(n), deg)
+    lo, hi = int(bounds[rank]), int(bounds[rank + 1])
+    own = (og.idx >= lo) & (og.idx < hi)
+    s_own, d_own = src[own], og.idx[own].astype(np.int64)
+    labels = np.arange(n, dtype=np.int32)
+    front = np.ones(n, np.uint8)
+    rounds = 0
+    while front.any():
+        act = front[s_own] == 1
+        best = labels.copy()
+        np.minimum.at(best, d_own[act], labels[s_own[act]])
+        nxt = np.zeros(n, np.uint8)
+        changed = best[lo:hi] < labels[lo:hi]
+        labels[lo:hi] = best[lo:hi]
+        nxt[lo:hi] = changed
+        ex(labels.ctypes.data, 4, list(bounds), None)
+        ex(nxt.ctypes.data, 1, list(bounds), None)
+        front = nxt
+        rounds += 1
+    return labels, rounds
+
+
 def _rank_main(rank, world, port, q):
     import datetime
     import torch.distributed as dist
@@ -81,12 +111,17 @@ def _rank_main(rank, world, port, q):
         bounds = partition_bounds(og.off, og.idx, world, row_work=ROW_WORK)
         pr = _pagerank_partitioned(og, bounds, rank, ex, 8)
         want = pm_oracle.pagerank(og, 8)
-        q.put((rank, ok_empty, ok_uneven, bounds.tolist(), bool(np.allclose(pr, want, rtol=1e-10, atol=0))))
+        sym = pm_oracle.rmat_graph(11, 8, symmetric=True)
+        sb = partition_bounds(sym.off, sym.idx, world, row_work=ROW_WORK)
+        lab, rounds = _components_partitioned(sym, sb, rank, ex)
+        same_cc = bool(np.array_equal(lab, pm_oracle.cc(sym)))
+        q.put((rank, ok_empty, ok_uneven, bounds.tolist(), bool(np.allclose(pr, want, rtol=1e-10, atol=0)),
+               same_cc, rounds))
     finally:
         dist.destroy_process_group()
 
 
-def test_partitioned_pagerank_two_gloo_ranks():
+def test_partitioned_pagerank_and_components_two_gloo_ranks():
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -100,5 +135,6 @@ def test_partitioned_pagerank_two_gloo_ranks():
     assert res[0][3] == res[1][3]  # both ranks cut the same ranges
     lo, mid, hi = res[0][3]
     assert lo == 0 and 0 < mid < hi and mid % 32 == 0
-    for rank, ok_empty, ok_uneven, _, same in res:
-        assert ok_empty and ok_uneven and same
+    for rank, ok_empty, ok_uneven, _, same, same_cc, rounds in res:
+        assert ok_empty and ok_uneven and same and same_cc
+    assert res[0][6] == res[1][6] > 1  # both ranks ended in the same round
