@@ -496,6 +496,19 @@ PM_API pm_status pm_host_free(void *p);
 /* Number of kernels this library launched since the last reset. */
 PM_API int64_t pm_kernel_launches(int reset);
 
+/* ---- failure tests (no reference counterpart: the reference aborts or
+ * prints and goes on).  Both fail on purpose, on the host's terms: nothing
+ * faults, traps or hangs a GPU.
+ * pm_test_fail_alloc_after(k): the k-th device allocation of the library
+ * from now on fails as an out-of-memory would (PM_ERR_OOM from the call that
+ * made it; the handle stays usable); k < 1 turns it off.
+ * pm_test_wait_timeout(device, max_polls): runs the bounded device wait the
+ * persistent kernels use (a poll every 256 ns, max_polls at most) on a flag
+ * that nothing sets; it gives up, the kernel returns, and the call returns
+ * PM_ERR_TIMEOUT with the device still usable.  max_polls in [1, 2^22]. */
+PM_API pm_status pm_test_fail_alloc_after(int64_t k);
+PM_API pm_status pm_test_wait_timeout(int device, int32_t max_polls);
+
 PM_API const char *pm_last_error(void);
 PM_API const char *pm_version(void);
 

@@ -144,6 +144,8 @@ def lib():
                                       C.POINTER(vp)],
         "pm_graph_set_exchange": [vp, EXCHANGE_FN, vp],
         "pm_graph_partition_info": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
+        "pm_test_fail_alloc_after": [i64],
+        "pm_test_wait_timeout": [C.c_int, i32],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -443,6 +445,18 @@ class Graph:
             _check(lib().pm_tune_mix(self._h, a.ctypes.data_as(C.c_void_p), len(a), C.byref(r)))
         return {"trials": r.trials, "default_ms": r.default_ms, "best_ms": r.best_ms,
                 "tunables": self.tunables()}
+
+
+def test_fail_alloc_after(k: int) -> None:
+    """Failure tests: the k-th device allocation of the library from now on
+    fails as an out-of-memory would (k < 1: off)."""
+    _check(lib().pm_test_fail_alloc_after(int(k)))
+
+
+def test_wait_timeout(max_polls: int, device: int = 0) -> None:
+    """Failure tests: a bounded device wait on a flag nothing sets; raises
+    PolymerError with status 4 (PM_ERR_TIMEOUT)."""
+    _check(lib().pm_test_wait_timeout(int(device), int(max_polls)))
 
 
 class PinnedArray:

@@ -10,6 +10,7 @@
 // it makes its own stream wait on the event (a GPU-side dependency, no host
 // wait), so host threads that drive distinct handles do not serialise.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -94,12 +95,22 @@ void release_all(Cache &c) {
 
 }  // namespace
 
+// Allocation-failure injection for tests: the k-th dev_alloc from now on
+// (k >= 1) fails as an out-of-memory would; -1: off.
+std::atomic<long long> g_fail_after{-1};
+
+void set_alloc_fail_after(long long k) { g_fail_after.store(k < 1 ? -1 : k); }
+
 AllocCtx alloc_ctx() { return t_ctx; }
 void set_alloc_ctx(AllocCtx c) { t_ctx = c; }
 
 void *dev_alloc(size_t bytes, size_t *cap, int *device) {
   Cache &c = cache();
   const size_t want = round_cap(bytes);
+  if (g_fail_after.load() > 0 && g_fail_after.fetch_sub(1) == 1) {
+    g_fail_after.store(-1);
+    fail(PM_ERR_OOM, "injected allocation failure (pm_test_fail_alloc_after) of " + std::to_string(want) + " bytes");
+  }
   int dev = 0;
   PM_CUDA(cudaGetDevice(&dev));
   Block b{nullptr, 0, dev, nullptr, false};

@@ -65,6 +65,12 @@ namespace pm {
 void set_last_error(const std::string &msg) { t_last_error = msg; }
 }  // namespace pm
 
+// The bounded wait of the fused heavy-row pull (wait_at_least) on a flag that
+// nothing sets: it must give up, report kErrTimeout and return.
+__global__ void k_test_wait(const int32_t *flag, unsigned *err, int max_polls) {
+  if (threadIdx.x == 0) wait_at_least(flag, 1, max_polls, err);
+}
+
 // Scratch slots used for staging at the boundary (the algorithms use 0..3).
 enum { kSlotIn0 = 8, kSlotIn1 = 9, kSlotOut0 = 10, kSlotOut1 = 11, kSlotAux = 12 };
 
@@ -984,6 +990,25 @@ pm_status pm_host_alloc(uint64_t bytes, void **out) {
 pm_status pm_host_free(void *p) {
   return guard([&] {
     if (p) PM_CUDA(cudaFreeHost(p));
+  });
+}
+
+pm_status pm_test_fail_alloc_after(int64_t k) {
+  return guard([&] { set_alloc_fail_after((long long)k); });
+}
+
+pm_status pm_test_wait_timeout(int device, int32_t max_polls) {
+  return guard([&] {
+    use_device(device);
+    need(max_polls >= 1 && max_polls <= kHeavyWaitSpins, "max_polls must be in [1, 2^22]");
+    DevBuf b(8);  // [0] the flag nothing sets, [1] the error word
+    PM_CUDA(cudaMemset(b.p, 0, 8));
+    PM_LAUNCH(k_test_wait, 1, 32, 0, (cudaStream_t)0, b.as<int32_t>(), reinterpret_cast<unsigned *>(b.as<int32_t>() + 1),
+              max_polls);
+    unsigned err = 0;
+    PM_CUDA(cudaMemcpy(&err, b.as<int32_t>() + 1, 4, cudaMemcpyDeviceToHost));
+    if (err & kErrTimeout)
+      fail(PM_ERR_TIMEOUT, "a bounded device wait ran out after " + std::to_string(max_polls) + " polls");
   });
 }
 

@@ -28,6 +28,8 @@ struct AllocCtx {
 PM_CXX_API AllocCtx alloc_ctx();
 PM_CXX_API void set_alloc_ctx(AllocCtx c);
 PM_CXX_API void *dev_alloc(size_t bytes, size_t *cap, int *device);
+// Tests: the k-th dev_alloc from now on fails with PM_ERR_OOM (k < 1: off).
+void set_alloc_fail_after(long long k);
 PM_CXX_API void dev_free(void *p, size_t cap, int device);
 // Small pinned host blocks, reused without cudaFreeHost (which synchronises
 // the device).

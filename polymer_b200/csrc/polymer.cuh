@@ -607,6 +607,21 @@ __device__ __forceinline__ int ld_acquire_gpu(const int32_t *p) {
 }
 constexpr int kHeavyWaitSpins = 1 << 22;  // x ~256 ns: gives up after about a second
 
+// Waits until *p >= target (acquire), at most max_spins polls 256 ns apart.
+// On giving up it sets kErrTimeout in *err and returns false: the kernel
+// goes on and the host turns the error word into PM_ERR_TIMEOUT.
+__device__ __forceinline__ bool wait_at_least(const int32_t *p, int32_t target, int max_spins, unsigned *err) {
+  int spins = 0;
+  while (ld_acquire_gpu(p) < target) {
+    if (++spins > max_spins) {
+      atomicOr(err, (unsigned)kErrTimeout);
+      return false;
+    }
+    __nanosleep(256);
+  }
+  return true;
+}
+
 // MODE 0: the partials of the heavy rows were summed by k_heavy_reduce
 // before this launch.  MODE 1 (fused): the first g.in.nchunks tickets are
 // heavy chunks, summed here by warp_heavy_chunk, and a heavy row's lane waits
@@ -790,14 +805,7 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
       const int first = __ldg(g.in.hfirst + r);
       const int nch = (deg + kChunkEdges - 1) / kChunkEdges;
       if constexpr (MODE == 1) {
-        int spins = 0;
-        while (ld_acquire_gpu(hdone + first) < nch) {
-          if (++spins > kHeavyWaitSpins) {
-            atomicOr(&cnt->err, (unsigned)kErrTimeout);
-            break;
-          }
-          __nanosleep(256);
-        }
+        wait_at_least(hdone + first, nch, kHeavyWaitSpins, &cnt->err);
         for (int k = 0; k < nch; ++k) acc = f.combine(acc, __ldcg(partials + first + k));
       } else {
         for (int k = 0; k < nch; ++k) acc = f.combine(acc, partials[first + k]);

@@ -98,6 +98,23 @@ def test_engine_api_compiles_outside_the_library():
     assert hasattr(L, "user_max_label")
 
 
+def test_failure_hooks_host_only():
+    """The allocation-failure injection is host state (set and cleared without
+    a GPU); the wait test needs a device and says so without one."""
+    import polymer_b200 as pm
+    pm.test_fail_alloc_after(3)
+    pm.test_fail_alloc_after(0)
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if not has_gpu:
+        with pytest.raises(pm.PolymerError) as ei:
+            pm.test_wait_timeout(10)
+        assert ei.value.status == 7  # PM_ERR_NO_DEVICE
+
+
 def test_memory_cache_settings_host_only():
     import polymer_b200 as pm
     pm.set_memory_cache(1 << 30)
