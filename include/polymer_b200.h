@@ -84,7 +84,18 @@ PM_API pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, i
  * that is not an integer or a value outside int32; PM_ERR_INVALID_ARG when a
  * file cannot be opened. */
 #define PM_LOAD_BINARY 16u
+/* With PM_LOAD_DUMP, path is a graph dump as dumpGraphToBin writes it and
+ * loadGraphFromBin reads it (IO-numa.h:758-900): int64 total bytes, int32 n,
+ * int64 m, then per vertex int32 words -1, id, out-degree, in-degree, the
+ * out-neighbours, the in-neighbours (at most 2^31 words).  Parsed on the GPU;
+ * PM_ERR_BAD_GRAPH for a wrong size, record count, id, degree or length. */
+#define PM_LOAD_DUMP 32u
 PM_API pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out);
+
+/* Write g as a graph dump (the layout of PM_LOAD_DUMP; dumpGraphToBin,
+ * IO-numa.h:837-900): the records are assembled on the device and written
+ * with one copy out.  Not for partition handles. */
+PM_API pm_status pm_graph_save_dump(pm_graph *g, const char *path);
 
 /* pm_graph_create with edge weights in CSR order (the weighted readers'
  * layout, readWghGraph IO-numa.h:318-402): wtype PM_I32 (BellmanFord) or

@@ -360,6 +360,61 @@ def write_binary(g: Graph, base: str) -> str:
     return base
 
 
+def transpose(g: Graph):
+    """In-adjacency of g: CSC offsets and, per destination, its sources in
+    ascending order (the order the reference's readGraph gives in-edges,
+    IO-numa.h:145-180)."""
+    deg = np.diff(g.off).astype(np.int64)
+    src = np.repeat(np.arange(g.n, dtype=np.int64), deg)
+    order = np.lexsort((src, g.idx.astype(np.int64)))
+    in_idx = src[order].astype(np.int32)
+    in_off = np.concatenate([[0], np.cumsum(np.bincount(g.idx, minlength=g.n))]).astype(np.int32)
+    return in_off, in_idx
+
+
+def write_dump(g: Graph, path: str) -> None:
+    """The graph dump of dumpGraphToBin (IO-numa.h:837-900): int64 total
+    bytes, int32 n, int64 m, then per vertex int32 -1, id, out-degree,
+    in-degree, out-neighbours, in-neighbours."""
+    in_off, in_idx = transpose(g)
+    parts = []
+    for v in range(g.n):
+        o0, o1, i0, i1 = g.off[v], g.off[v + 1], in_off[v], in_off[v + 1]
+        parts.append(np.array([-1, v, o1 - o0, i1 - i0], np.int32))
+        parts.append(g.idx[o0:o1].astype(np.int32))
+        parts.append(in_idx[i0:i1])
+    body = np.concatenate(parts).astype(np.int32).tobytes() if parts else b""
+    total = 8 + 4 + 8 + len(body)
+    with open(path, "wb") as f:
+        f.write(np.int64(total).tobytes() + np.int32(g.n).tobytes() + np.int64(len(g.idx)).tobytes() + body)
+
+
+def read_dump(path: str):
+    """The reader of loadGraphFromBin (IO-numa.h:758-830): (n, out_off,
+    out_idx, in_off, in_idx); raises ValueError where the reference aborts."""
+    raw = open(path, "rb").read()
+    total = int(np.frombuffer(raw[:8], np.int64)[0])
+    n = int(np.frombuffer(raw[8:12], np.int32)[0])
+    m = int(np.frombuffer(raw[12:20], np.int64)[0])
+    if total != len(raw):
+        raise ValueError("size")
+    w = np.frombuffer(raw[20:], np.int32)
+    p, out_off, in_off, outs, ins = 0, [0], [0], [], []
+    for v in range(n):
+        if w[p] != -1 or w[p + 1] != v:
+            raise ValueError("record %d" % v)
+        od, idg = int(w[p + 2]), int(w[p + 3])
+        outs.append(w[p + 4:p + 4 + od])
+        ins.append(w[p + 4 + od:p + 4 + od + idg])
+        out_off.append(out_off[-1] + od)
+        in_off.append(in_off[-1] + idg)
+        p += 4 + od + idg
+    if p != len(w) or out_off[-1] != m:
+        raise ValueError("length")
+    cat = lambda xs: np.concatenate(xs).astype(np.int32) if xs else np.zeros(0, np.int32)
+    return n, np.array(out_off, np.int32), cat(outs), np.array(in_off, np.int32), cat(ins)
+
+
 def write_text(g: Graph, path: str, w=None) -> None:
     wp = None if w is None else np.ascontiguousarray(w, np.int32)
     if lib().pmo_write_adj_text(path.encode(), g.n, g.off, _idx(g), _ptr(wp)) != 0:

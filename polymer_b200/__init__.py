@@ -32,7 +32,7 @@ __all__ = [
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_b200.so")
 
 PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
-PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY = 2, 4, 16
+PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY, PM_LOAD_DUMP = 2, 4, 16, 32
 # Work of one row in the pull's load balance and in the partition cut rule,
 # in edges (kRowWork of the kernels).
 ROW_WORK = 4
@@ -145,6 +145,7 @@ def lib():
         "pm_graph_set_exchange": [vp, EXCHANGE_FN, vp],
         "pm_graph_partition_info": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
         "pm_test_fail_alloc_after": [i64],
+        "pm_graph_save_dump": [vp, C.c_char_p],
         "pm_test_wait_timeout": [C.c_int, i32],
     }
     for name, args in sigs.items():
@@ -314,6 +315,20 @@ class Graph:
             | (PM_LOAD_BINARY if binary else 0)
         _check(lib().pm_graph_load_pbbs(os.fsencode(path), flags, device, C.byref(h)))
         return cls(h)
+
+    @classmethod
+    def load_dump(cls, path: str, symmetric: bool = False, skip_self_loops: bool = False,
+                  device: int = 0) -> "Graph":
+        """Read a graph dump (dumpGraphToBin's layout, parsed on the GPU)."""
+        h = C.c_void_p()
+        flags = (PM_GRAPH_SYMMETRIC if symmetric else 0) | (PM_GRAPH_SKIP_SELF_LOOPS if skip_self_loops else 0) \
+            | PM_LOAD_DUMP
+        _check(lib().pm_graph_load_pbbs(os.fsencode(path), flags, device, C.byref(h)))
+        return cls(h)
+
+    def save_dump(self, path: str) -> None:
+        """Write this graph as a graph dump (both adjacency directions)."""
+        _check(lib().pm_graph_save_dump(self._h, os.fsencode(path)))
 
     @classmethod
     def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 0x5EED0001, symmetric: bool = False,

@@ -15,7 +15,7 @@ OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libpolymer_b200.so")
 SOURCES = ["pm_engine.cu", "pm_graph.cu", "pm_apps.cu", "pm_batch.cu", "pm_adjoint.cu", "pm_capi.cu",
            "pm_static.cu", "pm_tune.cu", "pm_ingest.cu", "pm_alloc.cu", "pm_async.cu",
-           "pm_partition.cu", "pm_hubs.cu"]
+           "pm_partition.cu", "pm_hubs.cu", "pm_dump.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]

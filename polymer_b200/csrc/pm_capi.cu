@@ -12,6 +12,8 @@ long long launches(bool reset);
 void ingest_csr(pm_graph *g, bool skip_self_loops, DevBuf *w = nullptr);
 void parse_pbbs_text(pm_graph *g, const char *path, DevBuf &off, DevBuf &idx, DevBuf &w, int64_t &n,
                      int64_t &m);
+void read_graph_dump(pm_graph *g, const char *path, DevBuf &off, DevBuf &idx, int64_t &n, int64_t &m);
+void write_graph_dump(pm_graph *g, const char *path);
 void read_pbbs_binary(const char *base, std::vector<int32_t> &off, std::vector<int32_t> &idx, int64_t &n,
                       int64_t &m);
 void generate_rmat(pm_graph *g, int scale, int ef, uint64_t seed);
@@ -325,7 +327,9 @@ pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_gr
     try {
       DevBuf w;
       int64_t n = 0, m = 0;
-      if (flags & PM_LOAD_BINARY) {
+      if (flags & PM_LOAD_DUMP) {
+        read_graph_dump(g, path, g->out.off, g->out.idx, n, m);
+      } else if (flags & PM_LOAD_BINARY) {
         std::vector<int32_t> off, idx;
         read_pbbs_binary(path, off, idx, n, m);
         g->out.off.alloc((size_t)(n + 1) * 4);
@@ -349,6 +353,15 @@ pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_gr
       throw;
     }
     *out = g;
+  });
+}
+
+pm_status pm_graph_save_dump(pm_graph *g, const char *path) {
+  return guard([&] {
+    enter(g);
+    whole_graph(g, "pm_graph_save_dump");
+    need(path != nullptr, "null path");
+    write_graph_dump(g, path);
   });
 }
 

@@ -119,3 +119,49 @@ def test_create_weighted_skips_loops_with_their_weights(pm):
         o, i = g.csr()
         assert o.tolist() == [0, 1, 2, 3] and i.tolist() == [1, 2, 0]
         assert g.weights_i32().tolist() == [2, 3, 4]
+
+
+@pytest.mark.parametrize("sym", [False, True])
+def test_graph_dump_load_and_save(pm, oracle, tmp_path, sym):
+    """Graph dumps (dumpGraphToBin / loadGraphFromBin layout): the oracle's dump
+    loads into the oracle's CSR; the library's dump reads back, in the
+    oracle's reader, as the graph's CSR and its transpose."""
+    og = oracle.rmat_graph(11, 16, symmetric=sym)
+    path = str(tmp_path / "a.dump")
+    oracle.write_dump(og, path)
+    with pm.Graph.load_dump(path, symmetric=sym) as g:
+        assert same_csr(g, og)
+        if sym:
+            assert np.array_equal(pm.Components(g), oracle.cc(og))
+        out = str(tmp_path / "b.dump")
+        g.save_dump(out)
+    n, off, idx, in_off, in_idx = oracle.read_dump(out)
+    want_in_off, want_in_idx = oracle.transpose(og)
+    assert n == og.n and np.array_equal(off, og.off) and np.array_equal(idx, og.idx)
+    assert np.array_equal(in_off, want_in_off) and np.array_equal(in_idx, want_in_idx)
+    assert open(out, "rb").read() == open(path, "rb").read()  # the same bytes as the oracle's writer
+
+
+def test_graph_dump_malformed(pm, oracle, tmp_path):
+    og = oracle.rmat_graph(8, 4)
+    good = str(tmp_path / "g.dump")
+    oracle.write_dump(og, good)
+    raw = bytearray(open(good, "rb").read())
+
+    def bad(mutate, name):
+        b = bytearray(raw)
+        mutate(b)
+        p = str(tmp_path / name)
+        open(p, "wb").write(bytes(b))
+        with pytest.raises(pm.PolymerError) as ei:
+            pm.Graph.load_dump(p)
+        assert ei.value.status == 5, name
+
+    bad(lambda b: b.extend(b"\0\0\0\0"), "longer")                    # total size disagrees
+    bad(lambda b: b.__setitem__(slice(8, 12), np.int32(og.n + 1).tobytes()), "n")    # record count
+    bad(lambda b: b.__setitem__(slice(24, 28), np.int32(5).tobytes()), "id")         # record 0 says 5
+    bad(lambda b: b.__setitem__(slice(28, 32), np.int32(-3).tobytes()), "degree")    # negative degree
+    bad(lambda b: b.__setitem__(slice(12, 20), np.int64(len(og.idx) + 1).tobytes()), "m")  # m
+    with pytest.raises(pm.PolymerError) as ei:
+        pm.Graph.load_dump(str(tmp_path / "missing.dump"))
+    assert ei.value.status == 1

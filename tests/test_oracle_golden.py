@@ -164,3 +164,15 @@ def test_live_reference_scale12(oracle, tmp_path):
     par, cnt, _ = oracle.ref_bfs(bs, s, threads=4)
     depth, _ = oracle.bfs(gs, s)
     assert np.array_equal(oracle.bfs_depths_from_parents(par, s), depth)
+
+
+def test_oracle_graph_dump_round_trip(oracle, tmp_path):
+    """The oracle's restatement of dumpGraphToBin / loadGraphFromBin reads back
+    what it writes (both adjacency directions), on a directed graph."""
+    og = oracle.rmat_graph(9, 8)
+    path = str(tmp_path / "g.dump")
+    oracle.write_dump(og, path)
+    n, off, idx, in_off, in_idx = oracle.read_dump(path)
+    want_off, want_idx = oracle.transpose(og)
+    assert n == og.n and np.array_equal(off, og.off) and np.array_equal(idx, og.idx)
+    assert np.array_equal(in_off, want_off) and np.array_equal(in_idx, want_idx)
