@@ -176,6 +176,36 @@ def get_default_tunable(name: str) -> int:
     return v.value
 
 
+def save_tuning(path: str, tunables: dict, note: str = "") -> None:
+    """Persist a tuning table (e.g. Graph.tune(...)["tunables"] or
+    Graph.tunables()) as JSON, with a free-text note (the workload it was
+    tuned on)."""
+    import json
+    bad = sorted(set(tunables) - set(TUNABLES))
+    if bad:
+        raise PolymerError(1, "unknown tunables %s" % bad)
+    with open(path, "w") as f:
+        json.dump({"tunables": {k: int(v) for k, v in tunables.items()}, "note": note}, f, indent=1, sort_keys=True)
+
+
+def load_tuning(path: str, graph: "Graph | None" = None) -> dict:
+    """Apply a saved tuning table: to `graph`, or as the process-wide defaults
+    of graphs created afterwards (so tables that depend on them are built
+    once).  Returns the table."""
+    import json
+    with open(path) as f:
+        table = json.load(f)["tunables"]
+    bad = sorted(set(table) - set(TUNABLES))
+    if bad:
+        raise PolymerError(1, "unknown tunables %s" % bad)
+    for k, v in table.items():
+        if graph is None:
+            set_default_tunable(k, v)
+        else:
+            graph.set_tunable(k, v)
+    return table
+
+
 def set_memory_cache(max_bytes: int = -1) -> None:
     """Cap of the library's device-memory cache (-1: a quarter of the device, 0: off)."""
     _check(lib().pm_set_memory_cache(int(max_bytes)))

@@ -98,6 +98,23 @@ def test_engine_api_compiles_outside_the_library():
     assert hasattr(L, "user_max_label")
 
 
+def test_tuning_table_round_trip(tmp_path):
+    """A tuning table saved as JSON and loaded as process defaults (host
+    state, no GPU); unknown names are refused."""
+    import polymer_b200 as pm
+    before = {k: pm.get_default_tunable(k) for k in pm.TUNABLES}
+    path = str(tmp_path / "tuning.json")
+    try:
+        pm.save_tuning(path, {"heavy_deg": 512, "bfs_div": 64, "grid_expand": 256}, note="R-MAT 22 symmetric")
+        assert pm.load_tuning(path) == {"heavy_deg": 512, "bfs_div": 64, "grid_expand": 256}
+        assert pm.get_default_tunable("heavy_deg") == 512 and pm.get_default_tunable("bfs_div") == 64
+        with pytest.raises(pm.PolymerError):
+            pm.save_tuning(path, {"no_such_knob": 1})
+    finally:
+        for k, v in before.items():
+            pm.set_default_tunable(k, v)
+
+
 def test_failure_hooks_host_only():
     """The allocation-failure injection is host state (set and cleared without
     a GPU); the wait test needs a device and says so without one."""
