@@ -18,27 +18,56 @@ namespace pm {
 // the sources whose frontier contains v; visited[v] the sources that reached
 // v; depth[l * n + v] is v's level from source l.
 // Dense rounds: next[v] = OR of front over in-neighbours, minus visited[v]
-// (a pull-reduce with OR; commit records the new bits and their depth).
+// (a pull-reduce with OR; commit keeps the new bits).
 // Sparse rounds: every frontier vertex ORs its word into its out-neighbours'
-// next words; a vertexMap over the output queue then records them.
+// next words; a vertexMap over the output queue then masks them.
+// So next[v] ends every level as exactly the sources that reached v at that
+// level.  The levels' words stay in a ring of kMsbfsSlots-or-fewer slots and
+// the depths are written from them in tiles (k_msbfs_depths): one coalesced
+// pass over the k x n output instead of a fill plus one scattered 4-byte
+// store per (source, vertex).
 // ===========================================================================
 using u64 = unsigned long long;
 
-__device__ __forceinline__ void msbfs_record(u64 nb, int32_t *depth, int64_t n, int v, int32_t level) {
-  while (nb) {
-    const int l = __ffsll((long long)nb) - 1;
-    nb &= nb - 1;
-    depth[(int64_t)l * n + v] = level;
-  }
+constexpr int kMsbfsSlots = 16;     // level words kept before a flush
+constexpr int kMsbfsTile = 128;     // vertices per depth tile (one per thread)
+
+// Depths of the levels L0 .. L0+cnt-1, whose new-bits words sit in ring
+// slots (L0 + j) % slots.  first: no depth has been written yet, so the
+// block writes all k rows of its tile (-1 where no flushed level has the
+// lane) through shared memory, one 128-byte row segment per warp store;
+// otherwise only the lanes found are stored, straight to the output.
+__global__ void __launch_bounds__(kMsbfsTile) k_msbfs_depths(const u64 *__restrict__ ring, int slots,
+                                                             int32_t L0, int cnt, int k, int64_t n,
+                                                             bool first, int32_t *__restrict__ depth) {
+  __shared__ int32_t tile[64][kMsbfsTile];
+  const int t = threadIdx.x;
+  const int64_t v0 = (int64_t)blockIdx.x * kMsbfsTile;
+  const int64_t v = v0 + t;
+  if (first)
+    for (int l = 0; l < k; ++l) tile[l][t] = -1;
+  if (v < n)
+    for (int j = 0; j < cnt; ++j) {
+      u64 w = ring[(int64_t)((L0 + j) % slots) * n + v];
+      while (w) {
+        const int l = __ffsll((long long)w) - 1;
+        w &= w - 1;
+        if (first)
+          tile[l][t] = L0 + j;  // bank t % 32 whatever l is
+        else
+          depth[(int64_t)l * n + v] = L0 + j;
+      }
+    }
+  if (!first) return;
+  __syncthreads();
+  if (v < n)
+    for (int l = 0; l < k; ++l) depth[(int64_t)l * n + v] = tile[l][t];
 }
 
 struct MSBFS_F {
   const u64 *front;
   u64 *next;
   u64 *visited;
-  int32_t *depth;
-  int64_t n;
-  int32_t level;
   u64 full;
   using Acc = u64;
   __device__ __forceinline__ bool cond(int d) const { return *((volatile u64 *)visited + d) != full; }
@@ -54,40 +83,29 @@ struct MSBFS_F {
   __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
     const u64 nb = acc & ~visited[d];
     next[d] = nb;
-    if (nb) {
-      visited[d] |= nb;
-      msbfs_record(nb, depth, n, d, level);
-    }
+    if (nb) visited[d] |= nb;
     return nb != 0;
   }
 };
 
-// Records the bits that a sparse round ORed into next[v].
+// Keeps only the new bits that a sparse round ORed into next[v].
 struct MSBFS_Commit {
   u64 *next;
   u64 *visited;
-  int32_t *depth;
-  int64_t n;
-  int32_t level;
   __device__ __forceinline__ void operator()(int v) const {
     const u64 nb = next[v] & ~visited[v];
     next[v] = nb;
-    if (nb) {
-      visited[v] |= nb;
-      msbfs_record(nb, depth, n, v, level);
-    }
+    if (nb) visited[v] |= nb;
   }
 };
 
-__global__ void k_msbfs_seed(const int32_t *sources, int k, u64 *front, u64 *visited, uint32_t *bits,
-                             int32_t *depth, int64_t n) {
+__global__ void k_msbfs_seed(const int32_t *sources, int k, u64 *front, u64 *visited, uint32_t *bits) {
   const int l = threadIdx.x;
   if (l < k) {
     const int v = sources[l];
     atomicOr(front + v, 1ull << l);
     atomicOr(visited + v, 1ull << l);
     atomicOr(bits + (v >> 5), 1u << (v & 31));
-    depth[(int64_t)l * n + v] = 0;
   }
 }
 
@@ -112,31 +130,44 @@ void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, i
                pm_traversal_stats *st) {
   Engine &E = g->E;
   const int64_t n = g->n;
-  u64 *front = (u64 *)g->scratch_buf(0, (size_t)n * 8);
-  u64 *next = (u64 *)g->scratch_buf(1, (size_t)n * 8);
+  // Level t's new-bits words live in ring slot t % slots (about 1 GiB of
+  // ring at most, 3 slots at least: the front, the level being built, and
+  // one more so a flush never waits for every level).
+  const int slots = (int)std::max<int64_t>(3, std::min<int64_t>(kMsbfsSlots, (int64_t(1) << 30) / (8 * n)));
+  u64 *ring = (u64 *)g->scratch_buf(0, (size_t)n * 8 * slots);
   u64 *visited = (u64 *)g->scratch_buf(2, (size_t)n * 8);
-  PM_CUDA(cudaMemsetAsync(front, 0, (size_t)n * 8, E.stream));
+  auto slot = [&](int32_t t) { return ring + (int64_t)(t % slots) * n; };
+  PM_CUDA(cudaMemsetAsync(slot(0), 0, (size_t)n * 8, E.stream));
   PM_CUDA(cudaMemsetAsync(visited, 0, (size_t)n * 8, E.stream));
-  PM_CUDA(cudaMemsetAsync(d_depth, 0xff, (size_t)n * k * 4, E.stream));
   VertexSubset cur = g->subset(0), nxt = g->subset(1);
   PM_CUDA(cudaMemsetAsync(cur.bits, 0, cur.words() * 4, E.stream));
-  PM_LAUNCH(k_msbfs_seed, 1, 64, 0, E.stream, d_sources, k, front, visited, cur.bits, d_depth, n);
+  PM_LAUNCH(k_msbfs_seed, 1, 64, 0, E.stream, d_sources, k, slot(0), visited, cur.bits);
   cur.has_queue = false;
   subset_recount(E, cur);
   const u64 full = k == 64 ? ~0ull : ((1ull << k) - 1ull);
+  const unsigned tiles = (unsigned)((n + kMsbfsTile - 1) / kMsbfsTile);
+  int32_t flushed = 0;  // levels below this have their depths written
+  auto flush = [&](int32_t upto) {  // levels [flushed, upto]
+    PM_LAUNCH(k_msbfs_depths, tiles, kMsbfsTile, 0, E.stream, ring, slots, flushed, upto - flushed + 1, k, n,
+              flushed == 0, d_depth);
+    flushed = upto + 1;
+  };
   pm_traversal_stats s{};
   E.tag = "bfs_multi";
-  for (int32_t level = 1; cur.size > 0; ++level) {
+  int32_t level = 1;
+  for (; cur.size > 0; ++level) {
+    if (level - flushed == slots) flush(level - 1);  // slot(level) still holds an unwritten level
+    u64 *next = slot(level);
     PM_CUDA(cudaMemsetAsync(next, 0, (size_t)n * 8, E.stream));
     bool dense = false;
-    edgeMapReduce<int>(E, cur, MSBFS_F{front, next, visited, d_depth, n, level, full}, nxt, threshold,
-                       nullptr, nullptr, &dense);
-    if (!dense) vertexMap(E, nxt, MSBFS_Commit{next, visited, d_depth, n, level});
+    edgeMapReduce<int>(E, cur, MSBFS_F{slot(level - 1), next, visited, full}, nxt, threshold, nullptr, nullptr,
+                       &dense);
+    if (!dense) vertexMap(E, nxt, MSBFS_Commit{next, visited});
     s.rounds++;
     s.dense_rounds += dense;
-    std::swap(front, next);
     std::swap(cur, nxt);
   }
+  flush(level - 1);
   PM_CUDA(cudaMemsetAsync(E.d_cnt + 2, 0, sizeof(Counters), E.stream));
   PM_LAUNCH(k_msbfs_totals, E.grid_for(n, 256, 8), 256, 0, E.stream, visited, E.g.out.off, n, E.d_cnt + 2);
   const Counters *h = E.read_counters();

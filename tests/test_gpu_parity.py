@@ -198,6 +198,28 @@ def test_bfs_multi_matches_single_source(pm, oracle, threshold, sym, k):
     assert st["reached"] == reached and st["edges_visited"] == edges
 
 
+@pytest.mark.parametrize("threshold", [-1, 0])
+def test_bfs_multi_long_paths(pm, oracle, threshold):
+    """Hundreds of levels (more than the level words kept between depth
+    writes): a directed path 0 -> 1 -> ... -> 299 plus a separate 40-vertex
+    cycle, sources at both ends, inside, repeated, and on the cycle."""
+    n_path, n_cyc = 300, 40
+    n = n_path + n_cyc
+    src = np.r_[np.arange(n_path - 1), n_path + np.arange(n_cyc)]
+    dst = np.r_[np.arange(1, n_path), n_path + (np.arange(n_cyc) + 1) % n_cyc]
+    off = np.zeros(n + 1, np.int32)
+    np.add.at(off, src + 1, 1)
+    off = np.cumsum(off).astype(np.int32)
+    idx = dst[np.argsort(src, kind="stable")].astype(np.int32)
+    og = oracle.Graph(n, off, idx)
+    srcs = [0, 299, 150, 0, n_path + 7, 17, 1]
+    with pm.Graph.from_csr(off, idx) as g:
+        dep, st = pm.BFSMulti(srcs, g, threshold=threshold, stats=True)
+    for l, s in enumerate(srcs):
+        assert np.array_equal(dep[l], oracle.bfs(og, s)[0]), "lane %d" % l
+    assert st["rounds"] == n_path  # the longest walk (from 0) ends after 299 levels, plus the empty one
+
+
 def test_bfs_multi_device_out(pm, oracle):
     import torch
     og = oracle.rmat_graph(12, 16, symmetric=True)
