@@ -195,6 +195,8 @@ void run_msbfs(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_depth, i
 // fell is in the next frontier either way.
 // ===========================================================================
 constexpr int kLanes = 64;
+constexpr int kBfUnroll = 4;      // pull: in-edges whose row gathers are in flight together per warp
+constexpr int kBfPushUnroll = 2;  // push: out-edges whose target rows are read together per warp
 
 // active -> queue of frontier vertices with out-edges (and their degrees);
 // c->size = |F|, c->edges = outdeg(F), c->aux = queue length.
@@ -277,29 +279,42 @@ __global__ void __launch_bounds__(256) k_bf_multi_push(const int32_t *__restrict
     int cur = -1;
     u64 a = 0;
     int32_t slo = 0, shi = 0;
-    for (int j = 0; j < cnt; ++j) {
-      const int sj = __shfl_sync(0xffffffffu, s, j);
-      const int dj = __shfl_sync(0xffffffffu, d, j);
-      const int32_t wj = __shfl_sync(0xffffffffu, w, j);
-      if (sj != cur) {
-        cur = sj;
-        a = __ldg(active + sj);
-        slo = dist[(int64_t)sj * kLanes + lane];
-        shi = dist[(int64_t)sj * kLanes + 32 + lane];
+    for (int j0 = 0; j0 < cnt; j0 += kBfPushUnroll) {
+      // kBfPushUnroll edges at a time: the targets' rows are read, and their
+      // atomics issued, before any result is waited for.
+      int dj[kBfPushUnroll];
+      int32_t nlo[kBfPushUnroll], nhi[kBfPushUnroll], olo[kBfPushUnroll], ohi[kBfPushUnroll];
+#pragma unroll
+      for (int u = 0; u < kBfPushUnroll; ++u) {
+        const int j = min(j0 + u, cnt - 1);
+        const bool take = j0 + u < cnt;
+        const int sj = __shfl_sync(0xffffffffu, s, j);
+        dj[u] = __shfl_sync(0xffffffffu, d, j);
+        const int32_t wj = __shfl_sync(0xffffffffu, w, j);
+        if (sj != cur) {
+          cur = sj;
+          a = __ldg(active + sj);
+          slo = dist[(int64_t)sj * kLanes + lane];
+          shi = dist[(int64_t)sj * kLanes + 32 + lane];
+        }
+        nlo[u] = take && ((a >> lane) & 1ull) ? slo + wj : kDevBFInf;
+        nhi[u] = take && ((a >> (32 + lane)) & 1ull) ? shi + wj : kDevBFInf;
+        olo[u] = nlo[u] < kDevBFInf ? *(volatile int32_t *)(dist + (int64_t)dj[u] * kLanes + lane) : 0;
+        ohi[u] = nhi[u] < kDevBFInf ? *(volatile int32_t *)(dist + (int64_t)dj[u] * kLanes + 32 + lane) : 0;
       }
-      bool fell_lo = false, fell_hi = false;
-      if ((a >> lane) & 1ull) {
-        int32_t *p = dist + (int64_t)dj * kLanes + lane;
-        const int32_t nv = slo + wj;
-        if (nv < *(volatile int32_t *)p) fell_lo = nv < atomicMin(p, nv);
+#pragma unroll
+      for (int u = 0; u < kBfPushUnroll; ++u) {
+        if (nlo[u] < olo[u]) olo[u] = atomicMin(dist + (int64_t)dj[u] * kLanes + lane, nlo[u]);
+        else nlo[u] = kDevBFInf;
+        if (nhi[u] < ohi[u]) ohi[u] = atomicMin(dist + (int64_t)dj[u] * kLanes + 32 + lane, nhi[u]);
+        else nhi[u] = kDevBFInf;
       }
-      if ((a >> (32 + lane)) & 1ull) {
-        int32_t *p = dist + (int64_t)dj * kLanes + 32 + lane;
-        const int32_t nv = shi + wj;
-        if (nv < *(volatile int32_t *)p) fell_hi = nv < atomicMin(p, nv);
+#pragma unroll
+      for (int u = 0; u < kBfPushUnroll; ++u) {
+        const u64 mask = (u64)__ballot_sync(0xffffffffu, nlo[u] < olo[u]) |
+                         ((u64)__ballot_sync(0xffffffffu, nhi[u] < ohi[u]) << 32);
+        if (lane == 0 && mask) atomicOr(next_active + dj[u], mask);
       }
-      const u64 mask = (u64)__ballot_sync(0xffffffffu, fell_lo) | ((u64)__ballot_sync(0xffffffffu, fell_hi) << 32);
-      if (lane == 0 && mask) atomicOr(next_active + dj, mask);
     }
   }
 }
@@ -315,19 +330,33 @@ __device__ __forceinline__ void bf_multi_relax(const int32_t *__restrict__ in_id
     const int64_t e = base + lane;
     int s = 0;
     u64 act = 0;
+    int32_t w = 0;
     if (e < e1) {
       s = __ldg(in_idx + e);
       act = __ldg(active + s);
+      w = __ldg(w_in + e);
     }
     unsigned todo = __ballot_sync(0xffffffffu, act != 0);
+    // Up to kBfUnroll active in-edges per step: their row gathers are all
+    // issued before the first min consumes one.
     while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int sj = __shfl_sync(0xffffffffu, s, j);
-      const u64 aj = shfl_idx(act, j);
-      const int32_t wj = __ldg(w_in + base + j);
-      if ((aj >> lane) & 1ull) lo = min(lo, dist[(int64_t)sj * kLanes + lane] + wj);
-      if ((aj >> (32 + lane)) & 1ull) hi = min(hi, dist[(int64_t)sj * kLanes + 32 + lane] + wj);
+      int32_t vlo[kBfUnroll], vhi[kBfUnroll];
+#pragma unroll
+      for (int u = 0; u < kBfUnroll; ++u) {
+        const int j = todo ? __ffs(todo) - 1 : 0;
+        const bool take = todo != 0;
+        todo &= todo - 1;
+        const int sj = __shfl_sync(0xffffffffu, s, j);
+        const u64 aj = shfl_idx(act, j) & (take ? ~0ull : 0ull);
+        const int32_t wj = __shfl_sync(0xffffffffu, w, j);
+        vlo[u] = ((aj >> lane) & 1ull) ? dist[(int64_t)sj * kLanes + lane] + wj : kDevBFInf;
+        vhi[u] = ((aj >> (32 + lane)) & 1ull) ? dist[(int64_t)sj * kLanes + 32 + lane] + wj : kDevBFInf;
+      }
+#pragma unroll
+      for (int u = 0; u < kBfUnroll; ++u) {
+        lo = min(lo, vlo[u]);
+        hi = min(hi, vhi[u]);
+      }
     }
   }
 }
