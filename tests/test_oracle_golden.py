@@ -47,6 +47,32 @@ def test_pagerank_matches_reference_fixture(oracle):
     assert np.allclose(ours, ref, rtol=2e-9, atol=0)
 
 
+def test_pagerank_frontier_rule_is_not_textbook_pagerank(oracle):
+    """The reference's PageRank (numa-PageRank.C:273-335) updates only the
+    frontier and takes as the next frontier the targets of the current one,
+    so vertices with no in-edges drop out after the first iteration and keep
+    what sits in their slots.  A textbook all-vertex iteration (every vertex
+    gets 0.15/n + 0.85 * sum each iteration) is measurably different on the
+    same graph, while the oracle matches the reference's own output."""
+    z = load("rmat10_directed.npz")
+    n = len(z["off"]) - 1
+    g = oracle.Graph(n, z["off"], z["idx"])
+    src = np.repeat(np.arange(n), np.diff(z["off"]))
+    deg = np.diff(z["off"]).astype(np.float64)
+    p = np.full(n, 1.0 / n)
+    for _ in range(10):
+        contrib = np.where(deg > 0, p / np.maximum(deg, 1), 0.0)
+        q = np.zeros(n)
+        np.add.at(q, z["idx"], contrib[src])
+        p = 0.15 / n + 0.85 * q
+    ours = oracle.pagerank(g, 10)
+    assert np.allclose(ours, z["pagerank10"], rtol=2e-9, atol=0)
+    indeg = np.bincount(z["idx"], minlength=n)
+    assert (indeg == 0).sum() > 0  # the graph has vertices the frontier rule treats differently
+    rel = np.abs(p - ours).sum() / np.abs(ours).sum()
+    assert rel > 1e-3, rel
+
+
 def test_pagerank_skip_ring_fixture(oracle):
     z = load("tiny.npz")
     n = len(z["off"]) - 1
