@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "pm_graph.cuh"
 
 namespace pm {
@@ -76,8 +78,19 @@ __global__ void k_test_wait(const int32_t *flag, unsigned *err, int max_polls) {
 // Scratch slots used for staging at the boundary (the algorithms use 0..3).
 enum { kSlotIn0 = 8, kSlotIn1 = 9, kSlotOut0 = 10, kSlotOut1 = 11, kSlotAux = 12 };
 
+// One NVTX range per C-ABI call, named after the entry point, so a profiler
+// can select one application's kernels (ncu --nvtx --nvtx-include
+// "pm_pagerank/"); with no tool attached a push or pop is a pointer test.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 template <class Fn>
-static pm_status guard(Fn &&fn) {
+static pm_status guard(const char *name, Fn &&fn) {
+  NvtxRange range(name);
   AllocScope scope(AllocCtx{});  // enter() names the call's stream
   try {
     fn();
@@ -164,7 +177,7 @@ extern "C" {
 
 pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t n, int64_t m,
                           uint32_t flags, uint32_t mem, int device, pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
@@ -192,7 +205,7 @@ pm_status pm_graph_create(const int32_t *offsets, const int32_t *edges, int64_t 
 pm_status pm_graph_create_weighted(const int32_t *offsets, const int32_t *edges, const void *weights, int wtype,
                                    int64_t n, int64_t m, uint32_t flags, uint32_t mem, int device,
                                    pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
@@ -250,7 +263,7 @@ pm_status pm_graph_create_weighted(const int32_t *offsets, const int32_t *edges,
 pm_status pm_graph_create_partition(const int32_t *offsets, const int32_t *edges, const void *weights, int wtype,
                                     int64_t n, int64_t m, uint32_t flags, uint32_t mem, int rank, int nranks,
                                     int device, pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(n > 0 && n < (1ll << 31) - 1, "n must be in [1, 2^31-2]");
@@ -294,7 +307,7 @@ pm_status pm_graph_create_partition(const int32_t *offsets, const int32_t *edges
 }
 
 pm_status pm_graph_set_exchange(pm_graph *g, pm_allgather_fn fn, void *user) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     need(g->is_part, "not a partition graph");
     g->part_fn = fn;
@@ -303,7 +316,7 @@ pm_status pm_graph_set_exchange(pm_graph *g, pm_allgather_fn fn, void *user) {
 }
 
 pm_status pm_graph_partition_info(const pm_graph *g, int *rank, int *nranks, int64_t *bounds) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(g != nullptr, "null graph handle");
     if (rank) *rank = g->part_rank;
     if (nranks) *nranks = g->part_count;
@@ -319,7 +332,7 @@ pm_status pm_graph_partition_info(const pm_graph *g, int *rank, int *nranks, int
 }
 
 pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(path != nullptr, "null path");
@@ -357,7 +370,7 @@ pm_status pm_graph_load_pbbs(const char *path, uint32_t flags, int device, pm_gr
 }
 
 pm_status pm_graph_save_dump(pm_graph *g, const char *path) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_save_dump");
     need(path != nullptr, "null path");
@@ -367,7 +380,7 @@ pm_status pm_graph_save_dump(pm_graph *g, const char *path) {
 
 pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32_t flags, int device,
                                pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(scale >= 1 && scale <= 28, "scale must be in [1, 28]");
@@ -388,7 +401,7 @@ pm_status pm_graph_create_rmat(int scale, int edge_factor, uint64_t seed, uint32
 
 pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_max, int avg_degree,
                                    uint64_t seed, int device, pm_graph **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     need(count >= 1 && count <= 1 << 20, "count must be in [1, 2^20]");
@@ -407,7 +420,7 @@ pm_status pm_graph_create_er_batch(int count, int64_t n_min, int64_t n_max, int 
 }
 
 pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_set_parts");
     need(vbase != nullptr && count >= 1, "need count >= 1 part offsets");
@@ -418,7 +431,7 @@ pm_status pm_graph_set_parts(pm_graph *g, const int64_t *vbase, int count) {
 }
 
 pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(g != nullptr, "null graph handle");
     const int c = g->parts.empty() ? 0 : (int)g->parts.size() - 1;
     if (count) *count = c;
@@ -427,7 +440,7 @@ pm_status pm_graph_get_parts(pm_graph *g, int64_t *vbase, int *count) {
 }
 
 pm_status pm_pagerank_parts(pm_graph *g, int iters, double damping, float *ranks, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_pagerank_parts");
     check_mem(mem);
@@ -445,7 +458,7 @@ pm_status pm_pagerank_parts(pm_graph *g, int iters, double damping, float *ranks
 }
 
 pm_status pm_graph_destroy(pm_graph *g) {
-  return guard([&] {
+  return guard(__func__, [&] {
     if (!g) return;
     cudaSetDevice(g->device);
     delete g;
@@ -453,7 +466,7 @@ pm_status pm_graph_destroy(pm_graph *g) {
 }
 
 pm_status pm_graph_info(const pm_graph *g, int64_t *n, int64_t *m, int64_t *max_out_degree) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(g != nullptr, "null graph handle");
     if (n) *n = g->n;
     if (m) *m = g->m;
@@ -462,7 +475,7 @@ pm_status pm_graph_info(const pm_graph *g, int64_t *n, int64_t *m, int64_t *max_
 }
 
 pm_status pm_graph_get_csr(pm_graph *g, int32_t *offsets, int32_t *edges, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     if (offsets) from_device(g, offsets, g->out.off.p, (size_t)(g->n + 1) * 4, mem);
@@ -472,7 +485,7 @@ pm_status pm_graph_get_csr(pm_graph *g, int32_t *offsets, int32_t *edges, uint32
 }
 
 pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_set_weights_i32");
     check_mem(mem);
@@ -484,7 +497,7 @@ pm_status pm_graph_set_weights_i32(pm_graph *g, const int32_t *w, uint32_t mem) 
 }
 
 pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_set_weights_f32");
     check_mem(mem);
@@ -496,7 +509,7 @@ pm_status pm_graph_set_weights_f32(pm_graph *g, const float *w, uint32_t mem) {
 }
 
 pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_gen_weights_i32");
     need(wmax >= 1, "wmax must be >= 1");
@@ -505,7 +518,7 @@ pm_status pm_graph_gen_weights_i32(pm_graph *g, uint64_t seed, int32_t wmax) {
 }
 
 pm_status pm_graph_gen_weights_f32(pm_graph *g, uint64_t seed) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_gen_weights_f32");
     gen_weights(g, seed, 0, true);
@@ -513,7 +526,7 @@ pm_status pm_graph_gen_weights_f32(pm_graph *g, uint64_t seed) {
 }
 
 pm_status pm_graph_get_weights_f32(pm_graph *g, float *w, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(g->w_f32_out.p != nullptr, "graph has no float weights");
@@ -523,7 +536,7 @@ pm_status pm_graph_get_weights_f32(pm_graph *g, float *w, uint32_t mem) {
 }
 
 pm_status pm_graph_get_weights_i32(pm_graph *g, int32_t *w, uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(g->w_i32_out.p != nullptr, "graph has no int weights");
@@ -534,7 +547,7 @@ pm_status pm_graph_get_weights_i32(pm_graph *g, int32_t *w, uint32_t mem) {
 
 pm_status pm_fill_uniform_f32(pm_graph *g, uint64_t seed, int open_interval, float *out,
                               int64_t count) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     need(out != nullptr && count >= 0, "bad output");
     fill_uniform(g, seed, open_interval, out, count);
@@ -543,7 +556,7 @@ pm_status pm_fill_uniform_f32(pm_graph *g, uint64_t seed, int open_interval, flo
 
 pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uint32_t mem,
                  int64_t threshold, pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(src >= 0 && src < g->n, "source out of range");
@@ -558,7 +571,7 @@ pm_status pm_bfs(pm_graph *g, int32_t src, int32_t *parents, int32_t *depth, uin
 }
 
 pm_status pm_bfs_async(pm_graph *g, int32_t src, int32_t *parents, uint32_t mem, pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_bfs_async");
     check_mem(mem);
@@ -589,7 +602,7 @@ static const int32_t *stage_sources(pm_graph *g, const int32_t *sources, int k, 
 
 pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *depth, uint32_t mem,
                        int64_t threshold, pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_bfs_multi");
     check_mem(mem);
@@ -605,7 +618,7 @@ pm_status pm_bfs_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dept
 
 pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int32_t *dist, uint32_t mem,
                                 int64_t threshold, pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_bellman_ford_multi");
     check_mem(mem);
@@ -622,7 +635,7 @@ pm_status pm_bellman_ford_multi(pm_graph *g, const int32_t *sources, int k, int3
 
 pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t threshold,
                         pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(labels != nullptr, "null labels");
@@ -636,7 +649,7 @@ pm_status pm_components(pm_graph *g, int32_t *labels, uint32_t mem, int64_t thre
 
 pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem, int64_t threshold,
                           pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(dist != nullptr, "null dist");
@@ -652,7 +665,7 @@ pm_status pm_bellman_ford(pm_graph *g, int32_t src, int32_t *dist, uint32_t mem,
 
 pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *ranks, uint32_t mem,
                       double *resid) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     check_mem(mem);
     need(ranks != nullptr, "null ranks");
@@ -676,7 +689,7 @@ pm_status pm_pagerank(pm_graph *g, int iters, double damping, int dtype, void *r
 
 pm_status pm_pagerank_delta(pm_graph *g, int iters, double damping, double epsilon, int dtype, void *ranks,
                             uint32_t mem, int64_t threshold, pm_traversal_stats *stats) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_pagerank_delta");
     check_mem(mem);
@@ -701,7 +714,7 @@ pm_status pm_pagerank_delta(pm_graph *g, int iters, double damping, double epsil
 
 pm_status pm_ppr(pm_graph *g, const int32_t *seeds, int k, int iters, double damping, float *out,
                  uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_ppr");
     check_mem(mem);
@@ -751,11 +764,11 @@ static void spmv_call(pm_graph *g, const T *x0, int iters, T *y, uint32_t mem, d
 }  // extern "C++"
 
 pm_status pm_spmv(pm_graph *g, const float *x0, int iters, float *y, uint32_t mem, double *norm1) {
-  return guard([&] { spmv_call<float>(g, x0, iters, y, mem, norm1); });
+  return guard(__func__, [&] { spmv_call<float>(g, x0, iters, y, mem, norm1); });
 }
 
 pm_status pm_spmv_f64(pm_graph *g, const double *x0, int iters, double *y, uint32_t mem, double *norm1) {
-  return guard([&] { spmv_call<double>(g, x0, iters, y, mem, norm1); });
+  return guard(__func__, [&] { spmv_call<double>(g, x0, iters, y, mem, norm1); });
 }
 
 static void need_weights_f32(pm_graph *g) {
@@ -772,7 +785,7 @@ static const float *stage_in(pm_graph *g, const float *x, size_t count, int slot
 
 pm_status pm_weighted_pagerank(pm_graph *g, double damping, double tol, int max_iters, float *p,
                                uint32_t mem, int *iters, double *resid) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_weighted_pagerank");
     check_mem(mem);
@@ -791,7 +804,7 @@ pm_status pm_weighted_pagerank(pm_graph *g, double damping, double tol, int max_
 pm_status pm_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_iters, const float *p,
                               const float *grad_p, float *dw, float *lambda, uint32_t mem, int *iters,
                               double *resid) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_pagerank_adjoint");
     check_mem(mem);
@@ -816,7 +829,7 @@ pm_status pm_pagerank_adjoint(pm_graph *g, double damping, double tol, int max_i
 
 pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, float *dx, float *dw,
                            uint32_t mem) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_spmv_backward");
     check_mem(mem);
@@ -838,7 +851,7 @@ pm_status pm_spmv_backward(pm_graph *g, const float *x, const float *grad_y, flo
 }
 
 pm_status pm_graph_gen_weights_lognormal(pm_graph *g, uint64_t seed) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_graph_gen_weights_lognormal");
     gen_weights_lognormal(g, seed);
@@ -879,23 +892,23 @@ static void bp_call(pm_graph *g, const T *prior, const T *psi, int iters, T *log
 
 pm_status pm_bp(pm_graph *g, const float *prior, const float *psi, int iters, float *log_prod,
                 uint32_t mem) {
-  return guard([&] { bp_call<float>(g, prior, psi, iters, log_prod, mem); });
+  return guard(__func__, [&] { bp_call<float>(g, prior, psi, iters, log_prod, mem); });
 }
 
 pm_status pm_bp_f64(pm_graph *g, const double *prior, const double *psi, int iters, double *log_prod,
                     uint32_t mem) {
-  return guard([&] { bp_call<double>(g, prior, psi, iters, log_prod, mem); });
+  return guard(__func__, [&] { bp_call<double>(g, prior, psi, iters, log_prod, mem); });
 }
 
 pm_status pm_timer_begin(pm_graph *g) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     PM_CUDA(cudaEventRecord(g->ev0, g->E.stream));
   });
 }
 
 pm_status pm_timer_end(pm_graph *g, float *ms) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     PM_CUDA(cudaEventRecord(g->ev1, g->E.stream));
     PM_CUDA(cudaEventSynchronize(g->ev1));
@@ -906,7 +919,7 @@ pm_status pm_timer_end(pm_graph *g, float *ms) {
 }
 
 pm_status pm_profile_enable(pm_graph *g, int enable) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     g->E.prof.enabled = enable != 0;
   });
@@ -914,7 +927,7 @@ pm_status pm_profile_enable(pm_graph *g, int enable) {
 
 pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_t *passes,
                           int reset) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     need(tag != nullptr, "null tag");
     finish(g);
@@ -934,7 +947,7 @@ pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms, int64_
 }
 
 pm_status pm_graph_set_stream(pm_graph *g, void *stream) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     finish(g);  // nothing of this handle stays in flight on the old stream
     g->E.release_graphs();  // captured loops were recorded for the old stream's work
@@ -944,14 +957,14 @@ pm_status pm_graph_set_stream(pm_graph *g, void *stream) {
 }
 
 pm_status pm_graph_set_tunable(pm_graph *g, int key, int64_t value) {
-  return guard([&] {
+  return guard(__func__, [&] {
     if (g) enter(g);
     set_tunable(g, key, value);
   });
 }
 
 pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
-  return guard([&] {
+  return guard(__func__, [&] {
     if (g) enter(g);
     need(value != nullptr, "null value");
     *value = get_tunable(g, key);
@@ -959,7 +972,7 @@ pm_status pm_graph_get_tunable(pm_graph *g, int key, int64_t *value) {
 }
 
 pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_tune");
     tune(g, &app, 1, report);
@@ -968,7 +981,7 @@ pm_status pm_tune(pm_graph *g, int app, pm_tune_report *report) {
 }
 
 pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *report) {
-  return guard([&] {
+  return guard(__func__, [&] {
     enter(g);
     whole_graph(g, "pm_tune_mix");
     need(apps != nullptr, "null apps");
@@ -978,22 +991,22 @@ pm_status pm_tune_mix(pm_graph *g, const int *apps, int count, pm_tune_report *r
 }
 
 pm_status pm_set_memory_cache(int64_t max_bytes) {
-  return guard([&] { set_memory_cache(max_bytes); });
+  return guard(__func__, [&] { set_memory_cache(max_bytes); });
 }
 
 pm_status pm_release_memory_cache(void) {
-  return guard([&] { release_memory_cache(); });
+  return guard(__func__, [&] { release_memory_cache(); });
 }
 
 pm_status pm_memory_cache_info(int64_t *cached_bytes) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(cached_bytes != nullptr, "null cached_bytes");
     *cached_bytes = memory_cached();
   });
 }
 
 pm_status pm_host_alloc(uint64_t bytes, void **out) {
-  return guard([&] {
+  return guard(__func__, [&] {
     need(out != nullptr, "out is null");
     *out = nullptr;
     PM_CUDA(cudaMallocHost(out, bytes ? bytes : 1));
@@ -1001,17 +1014,17 @@ pm_status pm_host_alloc(uint64_t bytes, void **out) {
 }
 
 pm_status pm_host_free(void *p) {
-  return guard([&] {
+  return guard(__func__, [&] {
     if (p) PM_CUDA(cudaFreeHost(p));
   });
 }
 
 pm_status pm_test_fail_alloc_after(int64_t k) {
-  return guard([&] { set_alloc_fail_after((long long)k); });
+  return guard(__func__, [&] { set_alloc_fail_after((long long)k); });
 }
 
 pm_status pm_test_wait_timeout(int device, int32_t max_polls) {
-  return guard([&] {
+  return guard(__func__, [&] {
     use_device(device);
     need(max_polls >= 1 && max_polls <= kHeavyWaitSpins, "max_polls must be in [1, 2^22]");
     DevBuf b(8);  // [0] the flag nothing sets, [1] the error word
