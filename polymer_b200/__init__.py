@@ -29,7 +29,12 @@ __all__ = [
     "BeliefPropagation", "TraversalStats", "lib", "LIB_PATH", "kernel_launches",
 ]
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpolymer_b200.so")
+# POLYMER_B200_CHECKED=1 loads the checked build (every vertex id the engine
+# kernels read is bounds-tested; a bad one fails the call with
+# PM_ERR_BAD_GRAPH instead of reading out of bounds).
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        "libpolymer_b200_check.so" if os.environ.get("POLYMER_B200_CHECKED") == "1"
+                        else "libpolymer_b200.so")
 
 PM_MEM_HOST, PM_MEM_DEVICE = 0, 1
 PM_GRAPH_SYMMETRIC, PM_GRAPH_SKIP_SELF_LOOPS, PM_LOAD_BINARY, PM_LOAD_DUMP = 2, 4, 16, 32
@@ -83,7 +88,7 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise PolymerError(6, "libpolymer_b200.so is not built (run polymer_b200/_build.py)")
+        raise PolymerError(6, "%s is not built (run polymer_b200/_build.py)" % os.path.basename(LIB_PATH))
     L = C.CDLL(LIB_PATH)
     vp, i32, i64, u32, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64
     sigs = {

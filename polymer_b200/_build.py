@@ -13,6 +13,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libpolymer_b200.so")
+# The checked build: every vertex id the engine kernels read is bounds-tested
+# (PM_CHECK=1); loaded instead of LIB when POLYMER_B200_CHECKED=1.
+OBJ_CHECK = os.path.join(PKG, "_build_check")
+LIB_CHECK = os.path.join(PKG, "libpolymer_b200_check.so")
 SOURCES = ["pm_engine.cu", "pm_graph.cu", "pm_apps.cu", "pm_batch.cu", "pm_adjoint.cu", "pm_capi.cu",
            "pm_static.cu", "pm_tune.cu", "pm_ingest.cu", "pm_alloc.cu", "pm_async.cu",
            "pm_partition.cu", "pm_hubs.cu", "pm_dump.cu"]
@@ -33,16 +37,17 @@ def _stale(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, checked: bool = False) -> str:
+    obj_dir, lib = (OBJ_CHECK, LIB_CHECK) if checked else (OBJ, LIB)
+    os.makedirs(obj_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "polymer_b200.h"))
     nvcc = _nvcc()
-    extra = ["-Xptxas", "-v"] if ptxas_info else []
+    extra = (["-Xptxas", "-v"] if ptxas_info else []) + (["-DPM_CHECK=1"] if checked else [])
 
     def compile_one(src):
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src.replace(".cu", ".o"))
+        o = os.path.join(obj_dir, src.replace(".cu", ".o"))
         if force or ptxas_info or _stale(o, [s] + headers):
             cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", s, "-o", o]
             if verbose:
@@ -56,12 +61,12 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
 
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(compile_one, SOURCES))
-    if force or _stale(LIB, objs):
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    if force or _stale(lib, objs):
+        cmd = [nvcc, *ARCH, "-shared", "-o", lib, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n%s" % p.stderr)
-    return LIB
+    return lib
 
 
 def build_gather_probe() -> str:

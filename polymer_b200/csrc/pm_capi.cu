@@ -158,7 +158,17 @@ static void from_device(pm_graph *g, void *dst, const void *src, size_t bytes, u
                           mem == PM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                           g->E.stream));
 }
-static void finish(pm_graph *g) { PM_CUDA(cudaStreamSynchronize(g->E.stream)); }
+static void finish(pm_graph *g) {
+  PM_CUDA(cudaStreamSynchronize(g->E.stream));
+#if PM_CHECK
+  unsigned bad = 0;
+  if (g->check_word.p) {
+    PM_CUDA(cudaMemcpy(&bad, g->check_word.p, 4, cudaMemcpyDeviceToHost));
+    if (bad) PM_CUDA(cudaMemset(g->check_word.p, 0, 4));
+  }
+  if (bad) fail(PM_ERR_BAD_GRAPH, "checked build: a kernel read a vertex id outside [0, n)");
+#endif
+}
 static void check_mem(uint32_t mem) { need(mem == PM_MEM_HOST || mem == PM_MEM_DEVICE, "mem must be PM_MEM_HOST or PM_MEM_DEVICE"); }
 // The calls a partition graph serves: pm_pagerank, pm_spmv, pm_bp, pm_bfs,
 // pm_components, pm_bellman_ford (and the handle queries); the others need

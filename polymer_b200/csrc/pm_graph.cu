@@ -256,6 +256,13 @@ static void set_views(pm_graph *g) {
   v.heavy_deg = g->E.tune.heavy_deg;
   v.cta_expand = g->E.tune.cta_expand;
   v.grid_expand = g->E.tune.grid_expand;
+#if PM_CHECK
+  if (!g->check_word.p) {
+    g->check_word.alloc(16);
+    PM_CUDA(cudaMemsetAsync(g->check_word.p, 0, 16, g->E.stream));
+  }
+  v.check = g->check_word.as<unsigned>();
+#endif
 }
 
 void apply_tunables(pm_graph *g, int32_t old_heavy_deg) {

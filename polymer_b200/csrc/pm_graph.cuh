@@ -116,6 +116,7 @@ struct pm_graph : pm::IdleFreeBase {
   pm::Engine E;
   cudaStream_t own_stream = nullptr;  // created with the handle; E.stream may be a caller's
   pm::DevBuf cnt, bits0, bits1, queue0, queue1, defer, hubs, partials, hdone;
+  pm::DevBuf check_word;  // checked builds: set by a kernel that met an id outside [0, n)
   pm::Counters *h_cnt = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<pm::DevBuf> scratch;  // per-call workspaces kept across calls

@@ -65,6 +65,16 @@ struct Adj {
   int32_t nchunks = 0;
 };
 
+// Checked builds (-DPM_CHECK=1, libpolymer_b200_check.so; the stand-in for a
+// memory checker): a vertex id read from the graph or a queue is tested
+// against [0, n) before it indexes anything.  A bad one sets the graph's
+// check word and is replaced by vertex 0, so the kernel stays in bounds and
+// the call ends with PM_ERR_BAD_GRAPH.  Default builds compile the tests (and
+// the word) out: their kernels are the same code as without the option.
+#ifndef PM_CHECK
+#define PM_CHECK 0
+#endif
+
 struct GraphView {
   int32_t n = 0;
   int64_t m = 0;
@@ -73,7 +83,34 @@ struct GraphView {
   int32_t grid_expand = kGridExpand;
   Adj out;  // CSR
   Adj in;   // CSC (aliases out for symmetric graphs)
+#if PM_CHECK
+  unsigned *check = nullptr;  // the graph's bounds-check word
+#endif
 };
+__device__ __forceinline__ int checked_id(const GraphView &g, int v) {
+#if PM_CHECK
+  if ((unsigned)v >= (unsigned)g.n) {
+    atomicOr(g.check, 1u);
+    return 0;
+  }
+#endif
+  return v;
+}
+// A pull source: with the hub cache, ~s < hub_count names a cached hub.
+template <bool HUBS>
+__device__ __forceinline__ int checked_src(const GraphView &g, int hub_count, int s) {
+#if PM_CHECK
+  if (HUBS && s < 0) {
+    if (~s < hub_count) return s;
+    atomicOr(g.check, 1u);
+    return 0;
+  }
+  return checked_id(g, s);
+#else
+  (void)hub_count;
+  return s;
+#endif
+}
 
 __device__ __forceinline__ bool test_bit(const uint32_t *__restrict__ b, int v) {
   return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
@@ -153,7 +190,7 @@ __device__ __forceinline__ void emit_queue(bool act, int d, int32_t *queue, int3
 template <class F, class W>
 __device__ __forceinline__ bool push_edge(const GraphView &g, F &f, const W *w, int s, int64_t e,
                                           uint32_t *next_bits, int &d_out) {
-  int d = __ldg(g.out.idx + e);
+  int d = checked_id(g, __ldg(g.out.idx + e));
   d_out = d;
   if (f.cond(d) && f.updateAtomic(s, d, load_w(w, e))) return set_bit_new(next_bits, d);
   return false;
@@ -372,7 +409,7 @@ __global__ void __launch_bounds__(256) k_dense_pull(GraphView g, const uint32_t 
       int lim = min(o1, o0 + kPullScan);
       int e = o0;
       for (; e < lim; ++e) {
-        int s = __ldg(g.in.idx + e);
+        int s = checked_id(g, __ldg(g.in.idx + e));
         if (test_bit(cur, s) && f.updateAtomic(s, v, load_w(w, e))) act = true;
         if (!f.cond(v)) break;
       }
@@ -419,7 +456,7 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
     bool act = false, open = true;
     for (int base = o0; base < o1 && open; base += 32) {
       int e = base + lane;
-      int s = e < o1 ? __ldg(g.in.idx + e) : 0;
+      int s = e < o1 ? checked_id(g, __ldg(g.in.idx + e)) : 0;
       unsigned bal = __ballot_sync(0xffffffffu, e < o1 && test_bit(cur, s));
       while (bal && open) {
         int l = __ffs(bal) - 1;
@@ -542,7 +579,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_reduce(GraphView g, F f
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t e = e0 + threadIdx.x + (int64_t)u * kChunkThreads;
-      src[u] = e < e1 ? load_src(g.in.idx, w, e, wv[u]) : 0;
+      src[u] = e < e1 ? checked_id(g, load_src(g.in.idx, w, e, wv[u])) : 0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -582,7 +619,7 @@ __device__ __forceinline__ void warp_heavy_chunk(const GraphView &g, const F &f,
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int64_t e = base + 32 * u + lane;
-        src[u] = e < e1 ? load_src(g.in.idx, w, e, wv[u]) : 0;
+        src[u] = e < e1 ? checked_id(g, load_src(g.in.idx, w, e, wv[u])) : 0;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -716,7 +753,9 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
         typename EdgeT<W>::type wv[K];
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          src[k] = (32 * k + lane < cnt) ? load_src(lidx, w, (int64_t)e0 + 32 * k + lane, wv[k]) : 0;
+          src[k] = (32 * k + lane < cnt)
+                       ? checked_src<HUBS>(g, hubs.count, load_src(lidx, w, (int64_t)e0 + 32 * k + lane, wv[k]))
+                       : 0;
 #pragma unroll
         for (int k = 0; k < K; ++k)
           if (32 * k + lane < cnt)
@@ -747,7 +786,8 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
       }
       typename EdgeT<W>::type wv[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) src[k] = (q0 + k < total) ? load_src(lidx, w, es[k], wv[k]) : 0;
+      for (int k = 0; k < K; ++k)
+        src[k] = (q0 + k < total) ? checked_src<HUBS>(g, hubs.count, load_src(lidx, w, es[k], wv[k])) : 0;
       Acc vals[K];
 #pragma unroll
       for (int k = 0; k < K; ++k)
@@ -911,7 +951,7 @@ __global__ void __launch_bounds__(256) k_dense_push(GraphView g, const uint32_t 
       const int pj = __shfl_sync(0xffffffffu, pos, j);
       if (q < total) {
         const int64_t e = (int64_t)oj + (q - pj);
-        const int d = __ldg(g.out.idx + e);
+        const int d = checked_id(g, __ldg(g.out.idx + e));
         if (f.cond(d) && f.updateAtomic(rb + j, d, load_w(w, e)) && set_bit_new(next, d)) {
           my_size++;
           my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
@@ -942,7 +982,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_push(GraphView g,
   const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.out.off + r + 1));
   unsigned long long my_size = 0, my_edges = 0;
   for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads) {
-    const int d = __ldg(g.out.idx + e);
+    const int d = checked_id(g, __ldg(g.out.idx + e));
     if (f.cond(d) && f.updateAtomic(r, d, load_w(w, e)) && set_bit_new(next, d)) {
       my_size++;
       my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);

@@ -34,6 +34,17 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_checked_build_exports_every_declared_symbol():
+    """The bounds-checked build (PM_CHECK=1) is the same C ABI."""
+    import polymer_b200
+    path = os.path.join(os.path.dirname(polymer_b200.LIB_PATH), "libpolymer_b200_check.so")
+    if not os.path.exists(path):
+        pytest.skip("checked build not built (__graft_entry__.build())")
+    L = C.CDLL(path)
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+
+
 def test_version_string():
     import polymer_b200
     assert b"sm_100a" in polymer_b200.lib().pm_version()
