@@ -7,7 +7,6 @@ import socket
 import sys
 
 import numpy as np
-import pytest
 import torch.multiprocessing as mp
 
 from conftest import ROOT
