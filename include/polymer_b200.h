@@ -384,12 +384,18 @@ PM_API pm_status pm_bp_f64(pm_graph *g, const double *prior, const double *psi, 
  * vectors live in a fixed array inside the library, sized for at most
  * 1048576 vertices (about 8.3 MB, held on every GPU that loads the library
  * until the process exits); larger n is rejected with PM_ERR_INVALID_ARG.
- * Semantics are pm_pagerank's with PM_F32 (the graph must have no self
- * loops); pushes use atomics, so sums may differ from pm_pagerank in the
- * last bits.  Runs on `stream` (NULL = default stream) of the current device
- * and returns when done.  The first call on a device looks up the array's
- * address for that device; make it before any stream capture.  All calls on
- * a device share the array: calls that overlap on the GPU race. */
+ * Semantics are pm_pagerank's with PM_F32; pushes use atomics, so sums may
+ * differ from pm_pagerank in the last bits.  Each call first checks the CSR
+ * on the device and returns PM_ERR_BAD_GRAPH, computing nothing, when
+ * offsets are not monotone within [0, m], offsets[0] != 0, offsets[n] != m,
+ * an id lies outside [0, n) or an edge is a self loop.  Runs on `stream`
+ * (NULL = default stream) of the current device, reads a status word back
+ * after the check and after the last iteration, and returns when done.
+ * The first call on a device looks up the array's address for that device
+ * (and, with CUDA's lazy module loading, is when the array's memory is
+ * reserved): make it before any stream capture and before handing the
+ * device's free memory to another allocator.  All calls on a device share
+ * the array: calls that overlap on the GPU race. */
 PM_API pm_status pm_pagerank_static(const int32_t *offsets, const int32_t *edges, int64_t n,
                                     int64_t m, int iters, double damping, float *ranks,
                                     void *stream);

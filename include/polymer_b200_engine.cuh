@@ -38,6 +38,6 @@
 #define POLYMER_B200_ENGINE_CUH
 
 #include "polymer_b200.h"
-#include "../polymer_b200/csrc/pm_graph.cuh"
+#include "pm/pm_graph.cuh"
 
 #endif

@@ -32,14 +32,19 @@ SEED_SOURCES = 0x5EED0005
 
 _lib = None
 
+# Where the reference sources lie (read only by the build recipe; the one
+# place this path is set).  Absent on machines that only run the prebuilt
+# checkers.
+REFERENCE_DIR = os.environ.get("POLYMER_REFERENCE", "/root/reference")
+
 
 def build() -> None:
     """Compile the C restatement (and, when the reference sources are
     present, the reference binaries) with make."""
     targets = ["oracle"]
-    if os.path.isdir("/root/reference"):
+    if os.path.isdir(REFERENCE_DIR):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "REF=" + REFERENCE_DIR] + targets, check=True)
 
 
 def lib():

@@ -21,8 +21,10 @@ SOURCES = ["pm_engine.cu", "pm_graph.cu", "pm_apps.cu", "pm_batch.cu", "pm_adjoi
            "pm_static.cu", "pm_tune.cu", "pm_ingest.cu", "pm_alloc.cu", "pm_async.cu",
            "pm_partition.cu", "pm_hubs.cu", "pm_dump.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The engine's headers (the public template layer) live under include/pm.
+ENGINE_INC = os.path.join(ROOT, "include", "pm")
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
-         "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+         "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + ENGINE_INC, "-I" + CSRC]
 
 
 def _nvcc() -> str:
@@ -40,7 +42,7 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, checked: bool = False) -> str:
     obj_dir, lib = (OBJ_CHECK, LIB_CHECK) if checked else (OBJ, LIB)
     os.makedirs(obj_dir, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers = [os.path.join(d, f) for d in (CSRC, ENGINE_INC) for f in os.listdir(d) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "polymer_b200.h"))
     nvcc = _nvcc()
     extra = (["-Xptxas", "-v"] if ptxas_info else []) + (["-DPM_CHECK=1"] if checked else [])
@@ -67,15 +69,6 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, 
         if p.returncode != 0:
             raise RuntimeError("link failed:\n%s" % p.stderr)
     return lib
-
-
-def build_gather_probe() -> str:
-    """Standalone gather-rate probe (csrc/gather_probe.cu) -> polymer_b200/gather_probe."""
-    exe = os.path.join(PKG, "gather_probe")
-    src = os.path.join(CSRC, "gather_probe.cu")
-    if _stale(exe, [src]):
-        subprocess.run([_nvcc(), *ARCH, "-O3", "-o", exe, src], check=True)
-    return exe
 
 
 if __name__ == "__main__":

@@ -13,7 +13,7 @@ def build() -> str:
     src = os.path.join(HERE, "user_max_label.cu")
     deps = [src, os.path.join(ROOT, "include", "polymer_b200_engine.cuh"),
             os.path.join(ROOT, "polymer_b200", "libpolymer_b200.so")]
-    csrc = os.path.join(ROOT, "polymer_b200", "csrc")
+    csrc = os.path.join(ROOT, "include", "pm")
     deps += [os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith(".cuh")]
     if os.path.exists(OUT) and all(os.path.getmtime(d) <= os.path.getmtime(OUT) for d in deps):
         return OUT
