@@ -692,13 +692,19 @@ def SpMVBackward(g: Graph, x, grad_y):
 
 def PageRankStatic(offsets, edges, ranks, maxIter: int = 20, damping: float = 0.85, stream=None):
     """PageRank for callers that cannot allocate GPU memory (pm_pagerank_static):
-    offsets (n+1), edges (m) and ranks (n, float32) are CUDA tensors; the
-    working vectors live in a fixed array inside the library (n <= 2^20).
-    Nothing is allocated by this call."""
-    for t in (offsets, edges, ranks):
+    offsets (n+1 int32), edges (m int32) and ranks (n float32) are contiguous
+    CUDA tensors; the working vectors live in a fixed array inside the library
+    (n <= 2^20).  Nothing is allocated by this call."""
+    import torch
+    for t, dt, name in ((offsets, torch.int32, "offsets"), (edges, torch.int32, "edges"),
+                        (ranks, torch.float32, "ranks")):
         if not _is_device(t):
-            raise PolymerError(1, "PageRankStatic takes CUDA tensors only")
+            raise PolymerError(1, "PageRankStatic takes CUDA tensors only (%s)" % name)
+        if t.dtype != dt or not t.is_contiguous():
+            raise PolymerError(1, "%s must be a contiguous %s tensor" % (name, dt))
     n = offsets.numel() - 1
+    if ranks.numel() != n:
+        raise PolymerError(1, "ranks must hold offsets.numel() - 1 = %d floats" % n)
     _check(lib().pm_pagerank_static(C.c_void_p(offsets.data_ptr()), C.c_void_p(edges.data_ptr()), n,
                                     edges.numel(), int(maxIter), float(damping),
                                     C.c_void_p(ranks.data_ptr()),
