@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "pm_common.cuh"
@@ -187,12 +188,28 @@ __device__ __forceinline__ void emit_queue(bool act, int d, int32_t *queue, int3
 // Load balance: rows >= g.cta_expand are expanded by the whole CTA, rows >= 32
 // by one warp, the rest through a CTA-wide scan of their degrees.
 // ---------------------------------------------------------------------------
+// updateAtomic with the edge weight when the functor takes one
+// (polymer-wgh.h), without it otherwise (polymer.h's unweighted functors,
+// e.g. numa-Components.C:71-75).
+template <class F, class Wv, class = void>
+struct TakesWeight : std::false_type {};
+template <class F, class Wv>
+struct TakesWeight<F, Wv, std::void_t<decltype(std::declval<F &>().updateAtomic(0, 0, std::declval<Wv>()))>>
+    : std::true_type {};
+template <class F, class Wv>
+__device__ __forceinline__ bool update_atomic(F &f, int s, int d, Wv w) {
+  if constexpr (TakesWeight<F, Wv>::value)
+    return f.updateAtomic(s, d, w);
+  else
+    return f.updateAtomic(s, d);
+}
+
 template <class F, class W>
 __device__ __forceinline__ bool push_edge(const GraphView &g, F &f, const W *w, int s, int64_t e,
                                           uint32_t *next_bits, int &d_out) {
   int d = checked_id(g, __ldg(g.out.idx + e));
   d_out = d;
-  if (f.cond(d) && f.updateAtomic(s, d, load_w(w, e))) return set_bit_new(next_bits, d);
+  if (f.cond(d) && update_atomic(f, s, d, load_w(w, e))) return set_bit_new(next_bits, d);
   return false;
 }
 
@@ -410,7 +427,7 @@ __global__ void __launch_bounds__(256) k_dense_pull(GraphView g, const uint32_t 
       int e = o0;
       for (; e < lim; ++e) {
         int s = checked_id(g, __ldg(g.in.idx + e));
-        if (test_bit(cur, s) && f.updateAtomic(s, v, load_w(w, e))) act = true;
+        if (test_bit(cur, s) && update_atomic(f, s, v, load_w(w, e))) act = true;
         if (!f.cond(v)) break;
       }
       deferred = (e == lim) && lim < o1 && f.cond(v);
@@ -464,7 +481,7 @@ __global__ void __launch_bounds__(256) k_dense_pull_defer(GraphView g,
         int ss = __shfl_sync(0xffffffffu, s, l);
         int ok = 0, c = 1;
         if (lane == 0) {
-          ok = f.updateAtomic(ss, v, load_w(w, (int64_t)base + l));
+          ok = update_atomic(f, ss, v, load_w(w, (int64_t)base + l));
           c = f.cond(v);
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -914,6 +931,120 @@ __global__ void __launch_bounds__(256) k_heavy_commit(GraphView g, F f, const ty
 }
 
 // ---------------------------------------------------------------------------
+// Functors in the reference's own reducing-pull shape.  Polymer's
+// applications give edgeMapDenseReduce (polymer.h:1097-1168; weighted
+// polymer-wgh.h:951-1010) three members over a 16-byte scratch per vertex:
+//   initFunc(void *data, int d)
+//   reduceFunc(void *data, int s[, W w]) -> true when d is activated
+//   combineFunc(void *data, int d)
+// (numa-Components.C:77-99, numa-PageRank.C:98-119).  edgeMapReduce takes
+// such a functor as it is (the members __device__): its dense rounds run
+// k_pull_seq, which folds each vertex's frontier in-neighbours in CSC order
+// on one thread, exactly the reference's loop, because reduceFunc is a
+// sequential fold with no combine of two partial states.  Its sparse rounds
+// are the usual push with updateAtomic(s, d[, w]).  The reference's atomics
+// (utils.h:244-310) are below with the same names and results, so such a
+// functor's bodies compile unchanged apart from the __device__ qualifiers.
+// ---------------------------------------------------------------------------
+template <class F, class = void>
+struct RefReduceShape : std::false_type {};
+template <class F>
+struct RefReduceShape<F, std::void_t<decltype(std::declval<F &>().initFunc((void *)nullptr, 0)),
+                                     decltype(std::declval<F &>().combineFunc((void *)nullptr, 0))>>
+    : std::true_type {};
+
+template <class F, class Wv, class = void>
+struct ReduceTakesWeight : std::false_type {};
+template <class F, class Wv>
+struct ReduceTakesWeight<F, Wv,
+                         std::void_t<decltype(std::declval<F &>().reduceFunc((void *)nullptr, 0, std::declval<Wv>()))>>
+    : std::true_type {};
+template <class F, class Wv>
+__device__ __forceinline__ bool reduce_func(F &f, void *data, int s, Wv w) {
+  if constexpr (ReduceTakesWeight<F, Wv>::value)
+    return f.reduceFunc(data, s, w);
+  else
+    return f.reduceFunc(data, s);
+}
+
+// CAS / writeMin / writeAdd / fetchAndAdd of utils.h:244-310 on the GPU.
+template <class ET>
+__device__ __forceinline__ bool CAS(ET *ptr, ET oldv, ET newv) {
+  static_assert(sizeof(ET) == 4 || sizeof(ET) == 8, "CAS on 4- or 8-byte values");
+  if constexpr (sizeof(ET) == 8) {
+    unsigned long long o, nv;
+    memcpy(&o, &oldv, 8);
+    memcpy(&nv, &newv, 8);
+    return atomicCAS(reinterpret_cast<unsigned long long *>(ptr), o, nv) == o;
+  } else {
+    unsigned o, nv;
+    memcpy(&o, &oldv, 4);
+    memcpy(&nv, &newv, 4);
+    return atomicCAS(reinterpret_cast<unsigned *>(ptr), o, nv) == o;
+  }
+}
+// true when this call lowered *a to b
+template <class ET>
+__device__ __forceinline__ bool writeMin(ET *a, ET b) {
+  if constexpr (std::is_same<ET, int>::value || std::is_same<ET, unsigned>::value ||
+                std::is_same<ET, long long>::value || std::is_same<ET, unsigned long long>::value) {
+    return b < atomicMin(a, b);
+  } else {
+    ET c = *((volatile ET *)a);
+    while (c > b) {
+      if (CAS(a, c, b)) return true;
+      c = *((volatile ET *)a);
+    }
+    return false;
+  }
+}
+template <class ET>
+__device__ __forceinline__ void writeAdd(ET *a, ET b) {
+  atomicAdd(a, b);
+}
+template <class ET>
+__device__ __forceinline__ ET fetchAndAdd(ET *a, ET b) {
+  return atomicAdd(a, b);
+}
+
+template <class F, class W>
+__global__ void __launch_bounds__(256) k_pull_seq(GraphView g, const uint32_t *__restrict__ cur, F f,
+                                                  const W *__restrict__ w, uint32_t *__restrict__ next,
+                                                  Counters *cnt) {
+  const int lane = lane_id();
+  unsigned long long my_size = 0, my_edges = 0;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const int64_t ntot = ((int64_t)g.n + 31) & ~31ll;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += nthreads) {
+    const int v = (int)t;
+    bool act = false;
+    if (v < g.n && f.cond(v)) {
+      double data[2];  // the reference's per-vertex scratch (polymer.h:1140)
+      f.initFunc((void *)data, v);
+      const int o0 = __ldg(g.in.off + v), o1 = __ldg(g.in.off + v + 1);
+      for (int e = o0; e < o1; ++e) {
+        const int s = checked_id(g, __ldg(g.in.idx + e));
+        if (test_bit(cur, s) && reduce_func(f, (void *)data, s, load_w(w, e))) act = true;
+        if (!f.cond(v)) break;
+      }
+      if (o1 > o0) f.combineFunc((void *)data, v);
+    }
+    const unsigned word = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) next[v >> 5] = word;
+    if (act) {
+      my_size++;
+      my_edges += __ldg(g.out.off + v + 1) - __ldg(g.out.off + v);
+    }
+  }
+  my_size = warp_sum(my_size);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_size) {
+    atomicAdd(&cnt->size, my_size);
+    atomicAdd(&cnt->edges, my_edges);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Dense push (edgeMapDenseForward, polymer.h:970-1032): every vertex in the
 // frontier bitmap pushes over its out-edges with atomics; d's bit is set
 // when cond(d) && updateAtomic(s, d, w).  Same warp groups as the pull, over
@@ -952,7 +1083,7 @@ __global__ void __launch_bounds__(256) k_dense_push(GraphView g, const uint32_t 
       if (q < total) {
         const int64_t e = (int64_t)oj + (q - pj);
         const int d = checked_id(g, __ldg(g.out.idx + e));
-        if (f.cond(d) && f.updateAtomic(rb + j, d, load_w(w, e)) && set_bit_new(next, d)) {
+        if (f.cond(d) && update_atomic(f, rb + j, d, load_w(w, e)) && set_bit_new(next, d)) {
           my_size++;
           my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
         }
@@ -983,7 +1114,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_heavy_push(GraphView g,
   unsigned long long my_size = 0, my_edges = 0;
   for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads) {
     const int d = checked_id(g, __ldg(g.out.idx + e));
-    if (f.cond(d) && f.updateAtomic(r, d, load_w(w, e)) && set_bit_new(next, d)) {
+    if (f.cond(d) && update_atomic(f, r, d, load_w(w, e)) && set_bit_new(next, d)) {
       my_size++;
       my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
     }
@@ -1170,6 +1301,8 @@ struct Tunables {
                                      // 2 a launch beside it on a second stream
   int32_t hub_cache = 0;             // FP32 PageRank: sources cached in shared memory (0 = off)
   int32_t multi_div = 8;             // multi-source BFS / BellmanFord: default threshold = m / div
+  int32_t bf_dense = 0;              // BellmanFord dense rounds: 0 pull-reduce over the CSC,
+                                     // 1 push over the frontier's out-edges (DENSE_FORWARD)
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
@@ -1388,6 +1521,14 @@ void launch_dense_push(Engine &E, VertexSubset &cur, F f, const W *w_out, Vertex
   next.has_queue = false;
 }
 
+template <class W, class F>
+void launch_pull_seq(Engine &E, VertexSubset &cur, F f, const W *w_in, VertexSubset &next) {
+  const int64_t nthreads = ((int64_t)E.g.n + 31) & ~31ll;
+  PM_LAUNCH((k_pull_seq<F, W>), E.grid_for(nthreads, 256, 16), 256, 0, E.stream, E.g, cur.bits, f, w_in,
+            next.bits, E.d_cnt);
+  next.has_queue = false;
+}
+
 // Pull-reduce over the CSC into counters cnt (size / edges of the output,
 // daux = sum of the FP64 values commit() adds); next_bits may be null.
 template <class W, class F>
@@ -1481,7 +1622,9 @@ void edgeMap(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_t thre
 }
 
 // edgeMap with a reducing dense path (edgeMapCustom numa-Components.C:121-175
-// / edgeMapDenseReduce): dense rounds run the pull-reduce with fused commit,
+// / edgeMapDenseReduce): dense rounds run the pull-reduce with fused commit
+// (functors with identity / edge / combine / commit) or the reference's
+// sequential fold (functors with initFunc / reduceFunc / combineFunc),
 // sparse rounds the push with updateAtomic.
 template <class W = int, class F>
 void edgeMapReduce(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_t threshold,
@@ -1491,8 +1634,12 @@ void edgeMapReduce(Engine &E, VertexSubset &cur, F f, VertexSubset &next, int64_
   if (took_dense) *took_dense = dense;
   E.prof.begin(E.tag, E.stream);
   if (dense) {
-    launch_pull_reduce<W>(E, f, w_in, next.bits, E.d_cnt);
-    next.has_queue = false;
+    if constexpr (RefReduceShape<F>::value) {
+      launch_pull_seq<W>(E, cur, f, w_in, next);
+    } else {
+      launch_pull_reduce<W>(E, f, w_in, next.bits, E.d_cnt);
+      next.has_queue = false;
+    }
   } else {
     launch_sparse_push<W>(E, cur, f, w_out, next);
   }

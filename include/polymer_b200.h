@@ -453,6 +453,12 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
 #define PM_TUNE_MULTI_DIV 10       /* threshold < 0 means m / div: multi-source BFS and
                                       BellmanFord (default 8; their union frontiers turn
                                       dense sooner than one source's) */
+#define PM_TUNE_BF_DENSE 11        /* BellmanFord's dense rounds: 0 (default) a pull-reduce
+                                      over every in-edge (min of dist[s] + w over frontier
+                                      sources); 1 a push over the frontier's out-edges with
+                                      atomicMin, edgeMap's DENSE_FORWARD option, which the
+                                      reference's BellmanFord passes (numa-BellmanFord.C:182).
+                                      Ignored on a partition handle (pull only) */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

@@ -440,9 +440,11 @@ def _run(args, threads: int | None, timeout: float):
     return p.stdout, (float(t[-1][1]) if t else float("nan"))
 
 
-def ref_pagerank(path: str, iters: int, binary: bool = True, threads=None, result=True, timeout=600):
-    """numa-PageRank <g> <iters> -1 [-result] [-s] [-b]; returns (ranks|None, seconds)."""
-    args = [os.path.join(REF_DIR, "numa-PageRank"), path, str(iters), "-1",
+def ref_pagerank(path: str, iters: int, binary: bool = True, threads=None, result=True, timeout=600, exe=None):
+    """numa-PageRank <g> <iters> -1 [-result] [-s] [-b]; returns (ranks|None, seconds).
+    exe: another program with the same command line (the application built
+    with the B200 binding in place of its PageRank body)."""
+    args = [exe or os.path.join(REF_DIR, "numa-PageRank"), path, str(iters), "-1",
             "-result" if result else "-noresult", "-a", "-b" if binary else "-t"]
     out, t = _run(args, threads, timeout)
     if not result:

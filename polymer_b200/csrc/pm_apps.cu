@@ -378,10 +378,16 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
   s.reached = 1;
   const int32_t *w_out = g->w_i32_out.as<int32_t>(), *w_in = g->w_i32_in.as<int32_t>();
   E.tag = "bellman_ford";
+  // dense rounds: the pull-reduce, or the reference's dense push (DENSE_FORWARD,
+  // numa-BellmanFord.C:182), which reads only the frontier's out-edges
+  const bool push = E.tune.bf_dense == 1 && !g->is_part;
   while (cur.size > 0) {
     bool dense = false;
     s.edges_visited += cur.edges;
-    edgeMapReduce<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, w_out, w_in, &dense);
+    if (push)
+      edgeMap<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, &dense);
+    else
+      edgeMapReduce<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, w_out, w_in, &dense);
     part_exchange(g, d_dist, 4);  // a partition: distances and frontier of every rank
     part_round(g, next);
     s.rounds++;

@@ -2,7 +2,9 @@
 // with its own functors, compiled outside the library, as a Polymer application
 // is written against polymer.h: connected components by MAX-label propagation
 // (the mirror image of numa-Components.C's min labels), through edgeMapReduce
-// (sparse push or pull-reduce), vertexMapAll and a vertexFilter that counts
+// (sparse push or pull-reduce) or, with push != 0, edgeMap with the
+// DENSE_FORWARD option (sparse push or dense push over the frontier's
+// out-edges, updateAtomic only), vertexMapAll and a vertexFilter that counts
 // the component roots.  Test infrastructure: built and loaded by
 // tests/test_gpu_engine_api.py.
 #include <utility>
@@ -48,7 +50,7 @@ struct Root_F {
 
 // labels: n int32 on the graph's device.  Returns a pm_status.
 extern "C" __attribute__((visibility("default"))) int user_max_label(pm_graph *g, int32_t *labels,
-                                                                    int64_t threshold, int64_t *roots,
+                                                                    int64_t threshold, int push, int64_t *roots,
                                                                     int *rounds, int *dense_rounds) {
   try {
     PM_CUDA(cudaSetDevice(g->device));
@@ -59,7 +61,11 @@ extern "C" __attribute__((visibility("default"))) int user_max_label(pm_graph *g
     int r = 0, dr = 0;
     while (cur.size > 0) {
       bool dense = false;
-      pm::edgeMapReduce<int>(E, cur, MaxLabel_F{labels, cur.bits}, next, threshold, nullptr, nullptr, &dense);
+      if (push)
+        pm::edgeMap<int>(E, cur, MaxLabel_F{labels, cur.bits}, next, threshold, pm::DENSE_FORWARD, nullptr,
+                         nullptr, &dense);
+      else
+        pm::edgeMapReduce<int>(E, cur, MaxLabel_F{labels, cur.bits}, next, threshold, nullptr, nullptr, &dense);
       std::swap(cur, next);
       ++r;
       dr += dense;

@@ -261,6 +261,43 @@ def test_bellman_ford_exact(pm, oracle, threshold):
                 assert np.array_equal(d, oracle.dijkstra(og, w, int(s)))
 
 
+@pytest.mark.parametrize("threshold", [-1, 0])
+def test_bellman_ford_dense_push_exact(pm, oracle, threshold):
+    """Dense rounds through edgeMap's DENSE_FORWARD push (k_dense_push over
+    the frontier's out-edges, k_heavy_push for rows above the heavy cut-off),
+    the option the reference's BellmanFord passes (numa-BellmanFord.C:182):
+    distances equal Dijkstra's on R-MAT graphs of both kinds, with the heavy
+    cut-off at its default and lowered so that the chunk kernel runs."""
+    for sym, scale in ((True, 13), (False, 13)):
+        og = oracle.rmat_graph(scale, 16, symmetric=sym)
+        w = oracle.weights_int(og)
+        for heavy in (1024, 64):
+            with dev_graph(pm, og, symmetric=sym) as g:
+                g.set_weights(w)
+                g.set_tunable("bf_dense", 1)
+                g.set_tunable("heavy_deg", heavy)
+                for s in oracle.pick_sources(og, 3):
+                    d, st = pm.BellmanFord(g, int(s), threshold=threshold, stats=True)
+                    assert np.array_equal(d, oracle.dijkstra(og, w, int(s)))
+                    if threshold == 0:
+                        assert st["dense_rounds"] == st["rounds"]
+
+
+def test_bellman_ford_dense_push_hub(pm, oracle):
+    """A hub of in- and out-degree 12287 on a ring (three heavy chunks per
+    direction, a ragged last chunk): every round dense, pushed."""
+    n = 12288
+    src = np.concatenate([np.arange(1, n), np.zeros(n - 1, np.int64), np.arange(1, n - 1)])
+    dst = np.concatenate([np.zeros(n - 1, np.int64), np.arange(1, n), np.arange(2, n)])
+    og = oracle.graph_from_edges(n, src, dst)
+    w = oracle.weights_int(og)
+    with dev_graph(pm, og) as g:
+        g.set_weights(w)
+        g.set_tunable("bf_dense", 1)
+        for s in (5, 0, 7000, 12287):
+            assert np.array_equal(pm.BellmanFord(g, s, threshold=0), oracle.dijkstra(og, w, s))
+
+
 def _bf_multi_check(pm, oracle, og, sym, srcs, threshold):
     w = oracle.weights_int(og)
     with dev_graph(pm, og, symmetric=sym) as g:

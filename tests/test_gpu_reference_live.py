@@ -32,6 +32,25 @@ def test_pagerank_f64_scale16_vs_reference_binary(pm, oracle, tmp_path):
     assert np.allclose(r, ref, rtol=2e-9, atol=0)  # the reference prints %.9e
 
 
+BINDING = os.path.join(ROOT, "tests", "cpp", "_build", "numa-PageRank-b200")
+
+
+@pytest.mark.skipif(not os.path.exists(BINDING), reason="binding not built (reference sources absent at build time)")
+def test_reference_application_with_b200_binding(oracle, tmp_path):
+    """The reference's numa-PageRank.C with its PageRank body replaced by the
+    B200 binding (tests/cpp/ref_binding/pagerank_b200.inc, the text
+    INTEGRATION.md shows), run with the reference's own command line on the
+    2^16-vertex R-MAT of the FP64 PageRank workload: its -result output equals
+    the unmodified reference program's to the printed precision."""
+    og = oracle.rmat_graph(16, 16)
+    base = oracle.write_binary(og, str(tmp_path / "b16"))
+    got, t_b200 = oracle.ref_pagerank(base, 10, exe=BINDING)
+    ref, _ = oracle.ref_pagerank(base, 10)
+    assert len(got) == len(ref) == og.n
+    assert np.allclose(got, ref, rtol=2e-9, atol=0)
+    assert t_b200 == t_b200  # the application's own timer line was printed
+
+
 def test_components_and_bfs_scale22_vs_reference_binary(pm, oracle, tmp_path):
     with pm.Graph.rmat(22, 16, symmetric=True) as g:
         off, _ = g.csr()
