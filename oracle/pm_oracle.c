@@ -4,8 +4,12 @@
  * This file is the checker for the CUDA engine, never part of it: only the
  * tests, the smoke check and the CPU-baseline leg of the benchmark load it.
  * Every algorithm follows the reference application it cites, step by step,
- * in FP64 (or exact integers), single threaded, so that its results are
- * deterministic.  Parity of this restatement with the compiled reference is
+ * in FP64 (or exact integers), with every sum in a fixed order, so that its
+ * results are deterministic.  The value loops at scale (PageRank, SpMV, BP,
+ * PPR) run their push passes as pulls over the transpose, destinations in
+ * parallel (OpenMP): each destination still adds its in-neighbours'
+ * contributions in ascending source order, the order of the sequential push,
+ * so the results are bit-identical to it whatever the thread count.  Parity of this restatement with the compiled reference is
  * pinned by tests that run the reference binaries built from the original
  * sources (recipe in oracle/Makefile) on the same PBBS files.
  *
@@ -236,25 +240,42 @@ PMO_API void pmo_transpose(int64_t n, const int32_t *off, const int32_t *idx,
 /* The graph must be free of self loops (readGraphSkipRing, IO-numa.h:192).  */
 /* resid (optional) receives sum |p_{t+1} - p_t| for each iteration.          */
 /* ------------------------------------------------------------------------ */
+/* Transpose (CSC) with sources ascending per destination; *eid optional. */
+static void csc_alloc(int64_t n, const int32_t *off, const int32_t *idx, int32_t **toff, int32_t **tidx,
+                      int32_t **eid) {
+  int64_t m = off[n];
+  *toff = (int32_t *)malloc((size_t)(n + 1) * sizeof(int32_t));
+  *tidx = (int32_t *)malloc((size_t)(m > 0 ? m : 1) * sizeof(int32_t));
+  if (eid) *eid = (int32_t *)malloc((size_t)(m > 0 ? m : 1) * sizeof(int32_t));
+  pmo_transpose(n, off, idx, *toff, *tidx, eid ? *eid : NULL);
+}
+
 PMO_API void pmo_pagerank(int64_t n, const int32_t *off, const int32_t *idx, int iters,
                           double damping, double *out, double *resid) {
   double *pc = (double *)malloc((size_t)n * sizeof(double));
   double *pn = (double *)malloc((size_t)n * sizeof(double));
   unsigned char *F = (unsigned char *)malloc((size_t)n);
   unsigned char *Nx = (unsigned char *)malloc((size_t)n);
+  int32_t *toff, *tidx;
+  csc_alloc(n, off, idx, &toff, &tidx, NULL);
   double added = (1.0 - damping) * (1.0 / (double)n);
   for (int64_t i = 0; i < n; ++i) { pc[i] = 1.0 / (double)n; pn[i] = 0.0; F[i] = 1; }
   for (int it = 0; it < iters; ++it) {
-    memset(Nx, 0, (size_t)n);
-    for (int64_t s = 0; s < n; ++s) {
-      if (!F[s]) continue;
-      int64_t deg = off[s + 1] - off[s];
-      double val = pc[s];
-      for (int64_t e = off[s]; e < off[s + 1]; ++e) {
-        int32_t d = idx[e];
-        pn[d] += val / (double)deg;
-        Nx[d] = 1;
+    /* PR_F push, p_next[d] += p[s]/deg(s) for s in F, as a pull: d adds its */
+    /* frontier in-neighbours in ascending s; d joins the next frontier when */
+    /* it has one (edgeMapDenseForwardOTHER's next bit).                     */
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t d = 0; d < n; ++d) {
+      double acc = pn[d];
+      unsigned char hit = 0;
+      for (int64_t e = toff[d]; e < toff[d + 1]; ++e) {
+        int32_t s = tidx[e];
+        if (!F[s]) continue;
+        acc += pc[s] / (double)(off[s + 1] - off[s]);
+        hit = 1;
       }
+      pn[d] = acc;
+      Nx[d] = hit;
     }
     for (int64_t i = 0; i < n; ++i)
       if (F[i]) pn[i] = damping * pn[i] + added;
@@ -267,7 +288,7 @@ PMO_API void pmo_pagerank(int64_t n, const int32_t *off, const int32_t *idx, int
     unsigned char *tb = F; F = Nx; Nx = tb;
   }
   memcpy(out, pc, (size_t)n * sizeof(double));
-  free(pc); free(pn); free(F); free(Nx);
+  free(pc); free(pn); free(F); free(Nx); free(toff); free(tidx);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -328,14 +349,19 @@ PMO_API void pmo_ppr(int64_t n, const int32_t *off, const int32_t *idx, const in
                      int iters, double damping, double *out) {
   double *x = (double *)calloc((size_t)n * k, sizeof(double));
   double *y = (double *)malloc((size_t)n * k * sizeof(double));
+  int32_t *toff, *tidx;
+  csc_alloc(n, off, idx, &toff, &tidx, NULL);
   for (int j = 0; j < k; ++j) x[(int64_t)seeds[j] * k + j] = 1.0;
   for (int it = 0; it < iters; ++it) {
-    memset(y, 0, (size_t)n * k * sizeof(double));
-    for (int64_t s = 0; s < n; ++s) {
-      int64_t deg = off[s + 1] - off[s];
-      for (int64_t e = off[s]; e < off[s + 1]; ++e) {
-        int32_t d = idx[e];
-        for (int j = 0; j < k; ++j) y[(int64_t)d * k + j] += x[s * k + j] / (double)deg;
+    /* y[d] = sum over in-neighbours s (ascending) of x[s]/deg(s), per seed */
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t d = 0; d < n; ++d) {
+      double *yd = y + d * k;
+      for (int j = 0; j < k; ++j) yd[j] = 0.0;
+      for (int64_t e = toff[d]; e < toff[d + 1]; ++e) {
+        int32_t s = tidx[e];
+        double deg = (double)(off[s + 1] - off[s]);
+        for (int j = 0; j < k; ++j) yd[j] += x[(int64_t)s * k + j] / deg;
       }
     }
     for (int64_t i = 0; i < n * k; ++i) y[i] *= damping;
@@ -343,7 +369,7 @@ PMO_API void pmo_ppr(int64_t n, const int32_t *off, const int32_t *idx, const in
     double *t = x; x = y; y = t;
   }
   memcpy(out, x, (size_t)n * k * sizeof(double));
-  free(x); free(y);
+  free(x); free(y); free(toff); free(tidx);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -449,15 +475,21 @@ PMO_API void pmo_spmv(int64_t n, const int32_t *off, const int32_t *idx, const d
                       const double *x0, int iters, double *out) {
   double *x = (double *)malloc((size_t)n * sizeof(double));
   double *y = (double *)malloc((size_t)n * sizeof(double));
+  int32_t *toff, *tidx, *eid;
+  csc_alloc(n, off, idx, &toff, &tidx, &eid);
   memcpy(x, x0, (size_t)n * sizeof(double));
   for (int it = 0; it < iters; ++it) {
-    memset(y, 0, (size_t)n * sizeof(double));
-    for (int64_t s = 0; s < n; ++s)
-      for (int64_t e = off[s]; e < off[s + 1]; ++e) y[idx[e]] += x[s] * w[e];
+    /* SPMV_F push y[d] += x[s] * w_e as a pull, sources ascending */
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t d = 0; d < n; ++d) {
+      double acc = 0.0;
+      for (int64_t e = toff[d]; e < toff[d + 1]; ++e) acc += x[tidx[e]] * w[eid[e]];
+      y[d] = acc;
+    }
     double *t = x; x = y; y = t;
   }
   memcpy(out, x, (size_t)n * sizeof(double));
-  free(x); free(y);
+  free(x); free(y); free(toff); free(tidx); free(eid);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -620,32 +652,53 @@ PMO_API void pmo_bp(int64_t n, const int32_t *off, const int32_t *idx, const dou
   double *Ln = (double *)malloc((size_t)n * 2 * sizeof(double));
   unsigned char *F = (unsigned char *)malloc((size_t)n);
   unsigned char *Nx = (unsigned char *)malloc((size_t)n);
+  int32_t *toff, *tidx, *eid;
+  csc_alloc(n, off, idx, &toff, &tidx, &eid);
   for (int64_t i = 0; i < 2 * n; ++i) { Lc[i] = 0.0; Ln[i] = 0.0; }
   for (int64_t i = 0; i < n; ++i) F[i] = 1;
   for (int it = 0; it < iters; ++it) {
-    memset(Nx, 0, (size_t)n);
     for (int64_t i = 0; i < n; ++i)
       if (F[i]) { Ln[2 * i] = 0.0; Ln[2 * i + 1] = 0.0; }
-    for (int64_t s = 0; s < n; ++s) {
-      if (!F[s]) continue;
-      for (int64_t e = off[s]; e < off[s + 1]; ++e) {
-        int32_t d = idx[e];
-        const double *psi = psi_edge ? psi_edge + 4 * e : psi_uniform;
-        double l0 = Lc[2 * d], l1 = Lc[2 * d + 1];
-        double lm = l0 > l1 ? l0 : l1;
-        double a0 = prior[2 * d] * exp(l0 - lm), a1 = prior[2 * d + 1] * exp(l1 - lm);
-        double b0 = psi[0] * a0 + psi[1] * a1, b1 = psi[2] * a0 + psi[3] * a1;
-        double lz = log(b0 + b1);
-        Ln[2 * d] += log(b0) - lz;
-        Ln[2 * d + 1] += log(b1) - lz;
-        Nx[d] = 1;
+    /* the edge pass as a pull: d adds the message of every frontier        */
+    /* in-neighbour's edge in ascending source order.  The message of edge  */
+    /* s -> d depends on d's state and the edge's psi only; with a uniform  */
+    /* psi it is the same value for every in-edge of d and is computed once. */
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t d = 0; d < n; ++d) {
+      double l0 = Lc[2 * d], l1 = Lc[2 * d + 1];
+      double lm = l0 > l1 ? l0 : l1;
+      double a0 = prior[2 * d] * exp(l0 - lm), a1 = prior[2 * d + 1] * exp(l1 - lm);
+      double acc0 = Ln[2 * d], acc1 = Ln[2 * d + 1];
+      double u0 = 0.0, u1 = 0.0;
+      int have_u = 0;
+      unsigned char hit = 0;
+      for (int64_t e = toff[d]; e < toff[d + 1]; ++e) {
+        if (!F[tidx[e]]) continue;
+        double m0, m1;
+        if (psi_edge || !have_u) {
+          const double *psi = psi_edge ? psi_edge + 4 * (int64_t)eid[e] : psi_uniform;
+          double b0 = psi[0] * a0 + psi[1] * a1, b1 = psi[2] * a0 + psi[3] * a1;
+          double lz = log(b0 + b1);
+          m0 = log(b0) - lz;
+          m1 = log(b1) - lz;
+          if (!psi_edge) { u0 = m0; u1 = m1; have_u = 1; }
+        } else {
+          m0 = u0;
+          m1 = u1;
+        }
+        acc0 += m0;
+        acc1 += m1;
+        hit = 1;
       }
+      Ln[2 * d] = acc0;
+      Ln[2 * d + 1] = acc1;
+      Nx[d] = hit;
     }
     double *t = Lc; Lc = Ln; Ln = t;
     unsigned char *tb = F; F = Nx; Nx = tb;
   }
   memcpy(out_logprod, Lc, (size_t)n * 2 * sizeof(double));
-  free(Lc); free(Ln); free(F); free(Nx);
+  free(Lc); free(Ln); free(F); free(Nx); free(toff); free(tidx); free(eid);
 }
 
 /* ------------------------------------------------------------------------ */

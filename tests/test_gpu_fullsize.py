@@ -1,8 +1,8 @@
 """GPU parity at the benchmark's full sizes: every workload the benchmark
 times, on the same seeded inputs, against the CPU oracle (oracle/pm_oracle.c,
-FP64 / exact integers).  Slow: the oracle runs single-threaded per call, so
-the independent oracle computations of a graph run on a thread pool (the
-oracle's C calls release the GIL) while the GPU computes.
+FP64 / exact integers).  Slow: the oracle runs its value loops over all host
+cores (OpenMP) and the independent oracle computations of a graph run on a
+thread pool (its C calls release the GIL) while the GPU computes.
 
   symmetrised R-MAT scale 22 (graph A): the generator (CSR and int32 weights
     U{1..22}) bit-identical to the oracle's; BFS depths from all 16 seeded
@@ -42,7 +42,7 @@ def max_abs(a, b):
 
 @pytest.fixture(scope="module")
 def pool():
-    with cf.ThreadPoolExecutor(max_workers=8) as ex:
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
         yield ex
 
 
