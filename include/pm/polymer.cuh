@@ -1303,6 +1303,8 @@ struct Tunables {
   int32_t multi_div = 8;             // multi-source BFS / BellmanFord: default threshold = m / div
   int32_t bf_dense = 0;              // BellmanFord dense rounds: 0 pull-reduce over the CSC,
                                      // 1 push over the frontier's out-edges (DENSE_FORWARD)
+  int32_t cc_mode = 0;               // Components on a symmetric graph: 0 union-find,
+                                     // 1 label propagation (the reference's rounds)
 };
 
 // Key of a captured loop: its name and every value its launches bake in.

@@ -459,6 +459,13 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       atomicMin, edgeMap's DENSE_FORWARD option, which the
                                       reference's BellmanFord passes (numa-BellmanFord.C:182).
                                       Ignored on a partition handle (pull only) */
+#define PM_TUNE_CC_MODE 12         /* Components on a symmetric whole-graph handle: 0
+                                      (default) a concurrent union-find (sampled links,
+                                      the largest component skipped, roots are minimum
+                                      ids); 1 the reference's min-label propagation rounds
+                                      (threshold chooses their direction).  Same labels
+                                      either way; directed and partition handles always
+                                      propagate */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

@@ -19,7 +19,7 @@ OBJ_CHECK = os.path.join(PKG, "_build_check")
 LIB_CHECK = os.path.join(PKG, "libpolymer_b200_check.so")
 SOURCES = ["pm_engine.cu", "pm_graph.cu", "pm_apps.cu", "pm_batch.cu", "pm_adjoint.cu", "pm_capi.cu",
            "pm_static.cu", "pm_tune.cu", "pm_ingest.cu", "pm_alloc.cu", "pm_async.cu",
-           "pm_partition.cu", "pm_hubs.cu", "pm_dump.cu"]
+           "pm_partition.cu", "pm_hubs.cu", "pm_dump.cu", "pm_cc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # The engine's headers (the public template layer) live under include/pm.
 ENGINE_INC = os.path.join(ROOT, "include", "pm")

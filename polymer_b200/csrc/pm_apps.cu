@@ -310,7 +310,16 @@ __global__ void k_iota32(int32_t *a, int64_t n) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) a[v] = (int32_t)v;
 }
 
+void run_cc_union_find(pm_graph *g, int32_t *d_labels, pm_traversal_stats *st);
+
+// Symmetric whole-graph handles take the union-find of pm_cc.cu (the same
+// labels, PM_TUNE_CC_MODE 0, the default); directed graphs, partitions and
+// mode 1 run the reference's label propagation below.
 void run_cc(pm_graph *g, int32_t *d_labels, int64_t threshold, pm_traversal_stats *st) {
+  if (g->symmetric && !g->is_part && g->E.tune.cc_mode == 0) {
+    run_cc_union_find(g, d_labels, st);
+    return;
+  }
   Engine &E = g->E;
   VertexSubset cur = g->subset(0), next = g->subset(1);
   PM_LAUNCH(k_iota32, E.grid_for(g->n, 256, 16), 256, 0, E.stream, d_labels, g->n);

@@ -42,6 +42,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_HUB_CACHE: return t.hub_cache;
     case PM_TUNE_MULTI_DIV: return t.multi_div;
     case PM_TUNE_BF_DENSE: return t.bf_dense;
+    case PM_TUNE_CC_MODE: return t.cc_mode;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -89,6 +90,9 @@ void check_tunable(int key, int64_t value) {
       break;
     case PM_TUNE_BF_DENSE:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "bf_dense must be 0 or 1");
+      break;
+    case PM_TUNE_CC_MODE:
+      if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cc_mode must be 0 or 1");
       break;
     case PM_TUNE_HEAVY_MODE:
       if (value < 0 || value > 2) fail(PM_ERR_INVALID_ARG, "heavy_mode must be 0, 1 or 2");

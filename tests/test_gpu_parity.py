@@ -233,13 +233,45 @@ def test_bfs_multi_device_out(pm, oracle):
 
 
 # --------------------------------------------------------------------------
+@pytest.mark.parametrize("cc_mode", [0, 1])
 @pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
-def test_components_exact(pm, oracle, threshold):
+def test_components_exact(pm, oracle, threshold, cc_mode):
+    """Mode 0: union-find on symmetric graphs; mode 1: the reference's label
+    propagation in every direction regime.  Directed graphs always propagate."""
     for sym, scale in ((True, 13), (False, 12)):
         og = oracle.rmat_graph(scale, 8, symmetric=sym)
         with dev_graph(pm, og, symmetric=sym) as g:
-            lab = pm.Components(g, threshold=threshold)
+            g.set_tunable("cc_mode", cc_mode)
+            lab, st = pm.Components(g, threshold=threshold, stats=True)
         assert np.array_equal(lab, oracle.cc(og))
+        if sym and cc_mode == 0:
+            assert st["dense_rounds"] == 0 and st["edges_visited"] <= og.m
+
+
+def test_components_union_find_shapes(pm, oracle):
+    """Union-find against the oracle on shapes that stress linking: a long
+    path under a random vertex order (deep trees before compression), stars
+    whose centre has the largest id, many equal components (the sampled
+    largest component is one of several), isolated vertices."""
+    rng = np.random.default_rng(5)
+    n = 40000
+    perm = rng.permutation(n)
+    src, dst = [], []
+    path = perm[:20000]                       # one path over 20000 shuffled ids
+    src.append(path[:-1]); dst.append(path[1:])
+    for k in range(20):                       # 20 stars of 400 leaves, centre = largest id
+        ids = np.sort(perm[20000 + 500 * k: 20000 + 500 * k + 401])
+        src.append(np.full(400, ids[-1])); dst.append(ids[:-1])
+    for k in range(50):                       # 50 rings of 20 vertices
+        ids = perm[30100 + 20 * k: 30100 + 20 * k + 20]
+        src.append(ids); dst.append(np.roll(ids, 1))
+    og = oracle.graph_from_edges(n, np.concatenate(src), np.concatenate(dst), symmetric=True)
+    want = oracle.cc(og)
+    with dev_graph(pm, og, symmetric=True) as g:
+        for mode in (0, 1):
+            g.set_tunable("cc_mode", mode)
+            for _ in range(3):
+                assert np.array_equal(pm.Components(g), want), mode
 
 
 def test_components_reference_fixture(pm, oracle):
