@@ -120,6 +120,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def suite_config(scale_a, scale_b, n_sources, nA, mA, nB, mB, world):
+    """The workload both arms run (and report under `config`): the graphs and
+    applications of one step."""
+    return {
+        "workload": "six-application suite: BFS x%d + CC + BellmanFord on symmetrised R-MAT "
+                    "scale %d ef16 (n=%d, m=%d); PageRank 20 it + SpMV 10 it + BP 10 it on "
+                    "directed R-MAT scale %d ef16 (n=%d, m=%d)"
+                    % (n_sources, scale_a, nA, mA, scale_b, nB, mB),
+        "graphs": {"A": {"scale": scale_a, "n": nA, "m": mA}, "B": {"scale": scale_b, "n": nB, "m": mB}},
+        "l2": "inputs larger than L2 (126 MB): graph A ids %d MB, graph B ids %d MB" % (mA * 4 >> 20, mB * 4 >> 20),
+        "parallelism": "replicas x%d" % world,
+    }
+
+
 def _hash(seed, c):
     M = (1 << 64) - 1
     z = (seed + (c + 1) * 0x9E3779B97F4A7C15) & M
@@ -260,7 +274,8 @@ def errors_block(pm, suite):
     l32 = pm.BeliefPropagation(B, suite.prior, 10)
     l64 = pm.BeliefPropagation(B, suite.prior, 10, dtype=np.float64)
     out["bp_10it_logprod"] = err(l32, l64)
-    out["reference_precision"] = "FP64 on the GPU, same graph and inputs (tests pin it to the FP64 oracle)"
+    out["reference_precision"] = ("the GPU's own FP64 path on the same graph and inputs; the FP64 oracle "
+                                  "comparison at these sizes is tests/test_gpu_fullsize.py")
     return out
 
 
@@ -511,7 +526,9 @@ def batched_block(pm, suite, reps=3):
     t_pr = B.timer_end()
     nB, mB = B.n, B.m
     res["ppr32"] = {"ms": round(t_ppr, 3), "gteps": round(32 * 20 * mB / (t_ppr / 1e3) / 1e9, 2),
-                    "hbm_gbs": round(20 * (132 * mB + 136 * nB) / (t_ppr / 1e3) / 1e9, 1),
+                    "algorithmic_gbs": round(20 * (132 * mB + 264 * nB) / (t_ppr / 1e3) / 1e9, 1),
+                    "algorithmic_note": "132 m + 264 n bytes per iteration; the gathered 128-byte rows "
+                                        "mostly hit L2, so DRAM moves less (ncu summary in profiles/)",
                     "plain_32_vectors_ms": round(32 * t_pr, 3),
                     "speedup_vs_plain": round(32 * t_pr / t_ppr, 2),
                     "plain": "32 x one FP32 PageRank run of 20 iterations (one vector per run)"}
@@ -646,86 +663,6 @@ def ncu_traffic():
 # ---------------------------------------------------------------------------
 # CPU side: the reference binaries (oracle/_ref) or the oracle port.
 # ---------------------------------------------------------------------------
-class CpuSample:
-    """Bounded sample of the suite for the CPU: the same applications and
-    edge-count rules on smaller graphs (scale given), files written once."""
-
-    def __init__(self, scale, n_sources=2, wscale=None):
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pm_oracle as O
-        self.O = O
-        self.scale = scale
-        self.wscale = wscale or scale
-        self.d = O.tempdir()
-        self.gd = O.rmat_graph(scale, 16)
-        self.gs = O.rmat_graph(scale, 16, symmetric=True)
-        self.gdw = self.gd if self.wscale == scale else O.rmat_graph(self.wscale, 16)
-        self.gsw = self.gs if self.wscale == scale else O.rmat_graph(self.wscale, 16, symmetric=True)
-        self.kind = "reference" if O.ref_available() else "port"
-        self.sources = [int(s) for s in O.pick_sources(self.gs, n_sources)]
-        self.bf_src = int(O.pick_sources(self.gsw, 1)[0])
-        deg = np.diff(self.gs.off)
-        self.bfs_edges = []
-        for s in self.sources:
-            depth, _ = O.bfs(self.gs, s)
-            self.bfs_edges.append(int(deg[depth >= 0].sum()))
-        if self.kind == "reference":
-            self.bd = O.write_binary(self.gd, os.path.join(self.d, "dir"))
-            self.bs = O.write_binary(self.gs, os.path.join(self.d, "sym"))
-            self.tw_sym = os.path.join(self.d, "symw.txt")
-            O.write_text(self.gsw, self.tw_sym, O.weights_int(self.gsw))
-            # the reference SpMV reads int weights (numa-SPMV.C:72); same graph, U{1..22}
-            self.tw_dir = os.path.join(self.d, "dirw.txt")
-            O.write_text(self.gdw, self.tw_dir, O.weights_int(self.gdw))
-        else:
-            self.w_sym = O.weights_int(self.gsw)
-            self.w_dir = O.weights_unit(self.gdw).astype(np.float64)
-            self.x0 = O.uniform01(self.gdw.n).astype(np.float64)
-            self.prior = O.uniform_open(2 * self.gd.n).reshape(-1, 2).astype(np.float64)
-
-    def describe(self):
-        return ("R-MAT scale %d (PageRank 20 it, BP 10 it; BFS x%d, CC on the symmetrised graph), "
-                "scale %d weighted (SpMV 10 it, BellmanFord x1)" % (self.scale, len(self.sources),
-                                                                    self.wscale))
-
-    def step(self, threads):
-        """Runs the sample once; returns (seconds, edges, per-algo dict)."""
-        O = self.O
-        per = {}
-        if self.kind == "reference":
-            _, t = O.ref_pagerank(self.bd, 20, threads=threads, result=False)
-            per["pagerank"] = (t, self.gd.m * 20)
-            t = O.ref_bp(self.bd, 10, threads=threads)
-            per["bp"] = (t, self.gd.m * 10)
-            _, t = O.ref_spmv(self.tw_dir, 10, threads=threads, result=False)
-            per["spmv"] = (t, self.gdw.m * 10)
-            tb = 0.0
-            for s in self.sources:
-                _, _, t = O.ref_bfs(self.bs, s, threads=threads, parents=False)
-                tb += t
-            per["bfs"] = (tb, sum(self.bfs_edges))
-            _, t = O.ref_components(self.bs, threads=threads, result=False)
-            per["cc"] = (t, self.gs.m)
-            _, t = O.ref_bellman_ford(self.tw_sym, self.bf_src, threads=threads)
-            per["bellman_ford"] = (t, self.gsw.m)
-        else:
-            def timed(fn):
-                t0 = time.perf_counter()
-                fn()
-                return time.perf_counter() - t0
-            per["pagerank"] = (timed(lambda: O.pagerank(self.gd, 20)), self.gd.m * 20)
-            per["bp"] = (timed(lambda: O.bp(self.gd, self.prior, 10)), self.gd.m * 10)
-            per["spmv"] = (timed(lambda: O.spmv(self.gdw, self.w_dir, self.x0, 10)), self.gdw.m * 10)
-            per["bfs"] = (sum(timed(lambda s=s: O.bfs(self.gs, s)) for s in self.sources),
-                          sum(self.bfs_edges))
-            per["cc"] = (timed(lambda: O.cc(self.gs)), self.gs.m)
-            per["bellman_ford"] = (timed(lambda: O.bellman_ford(self.gsw, self.w_sym, self.bf_src)),
-                                   self.gsw.m)
-        secs = sum(v[0] for v in per.values())
-        edges = sum(v[1] for v in per.values())
-        return secs, edges, per
-
-
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -733,47 +670,138 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline():
+class RefSample:
+    """The reference programs (oracle/_ref, built from the unmodified sources,
+    all host threads, their own nextTime timers, graph loading excluded) on
+    the benchmark's own graphs: the symmetrised R-MAT A and the directed
+    R-MAT B, generated by the oracle (bit-identical to the device generator)
+    and written as the reference's binary graph files.
+
+    One step is a fixed subset of the suite: one PageRank iteration on B
+    (one process runs all iterations after a single load of B, 24 s at scale
+    24; the per-iteration time is its timer over the iteration count) and
+    one Components run or one BFS, alternating, on A (the BFS source cycles
+    through the suite's 16 sources).  BP (5.9 s per iteration at scale 24 on 8
+    cores, and no output), SpMV and BellmanFord (their reference inputs are
+    weighted text files of 1.3-2.6 GB whose parsing outlasts the rest; the
+    reference BellmanFord is also not exact) are left out."""
+
+    def __init__(self, scale_a, scale_b, n_sources=16, b_graph=True):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pm_oracle as O
+        self.O = O
+        if not O.ref_available():
+            raise RuntimeError("reference binaries not built (make -C oracle ref)")
+        self.d = O.tempdir()
+        ga = O.rmat_graph(scale_a, 16, seed=SEED_GRAPH, symmetric=True)
+        self.nA, self.mA = ga.n, ga.m
+        self.sources = pick_sources(ga.off, n_sources, SEED_SRC)
+        self.bfs_edges = {}
+        deg = np.diff(ga.off)
+        for s in self.sources:
+            self.bfs_edges[s] = int(deg[O.bfs(ga, s)[0] >= 0].sum())
+        self.fa = O.write_binary(ga, os.path.join(self.d, "a"))
+        del ga
+        self.nB = self.mB = None
+        if b_graph:
+            gb = O.rmat_graph(scale_b, 16, seed=SEED_GRAPH)
+            self.nB, self.mB = gb.n, gb.m
+            self.fb = O.write_binary(gb, os.path.join(self.d, "b"))
+            del gb
+
+    def run(self, warmup, steps, threads):
+        """(seconds, edges, per-application [seconds, edges]) of the timed
+        steps; warm-up steps run the same programs untimed."""
+        O = self.O
+        per = {}
+        tot_s, tot_e = 0.0, 0
+
+        def add(k, secs, edges):
+            nonlocal tot_s, tot_e
+            a = per.setdefault(k, [0.0, 0])
+            a[0] += secs
+            a[1] += edges
+            tot_s += secs
+            tot_e += edges
+
+        for i in range(warmup + steps):
+            if i % 2 == 0:
+                _, t = O.ref_components(self.fa, threads=threads, result=False)
+                k, e = "cc", self.mA
+            else:
+                s = self.sources[(i // 2) % len(self.sources)]
+                _, _, t = O.ref_bfs(self.fa, s, threads=threads, parents=False)
+                k, e = "bfs", self.bfs_edges[s]
+            if i >= warmup:
+                add(k, t, e)
+        if self.mB is not None:
+            _, t = O.ref_pagerank(self.fb, warmup + steps, threads=threads, result=False, timeout=3600)
+            add("pagerank", t * steps / (warmup + steps), self.mB * steps)
+        return tot_s, tot_e, per
+
+    def describe(self, steps):
+        parts = ["per step: Components or BFS (alternating; sources cycle through the suite's 16) on "
+                 "symmetrised R-MAT A"]
+        if self.mB is not None:
+            parts.append("one PageRank iteration on directed R-MAT B (one process, %d iterations after one "
+                         "load, per-iteration time from its timer)" % steps)
+        return "; ".join(parts) + ("; BP, SpMV and BellmanFord not in the sample; the reference binaries "
+                                   "with their own timers (graph loading excluded)")
+
+
+def cpu_baseline(suite):
+    """The reference programs on graph A of the timed suite (rank 0 at N=1):
+    one Components run and two BFS, their own timers, all host threads."""
     threads = cpu_threads()
-    s = CpuSample(18, n_sources=2, wscale=17)
-    secs, edges, per = s.step(threads if s.kind == "reference" else 1)
-    return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS",
-            "cores": threads if s.kind == "reference" else 1, "kind": s.kind,
-            "sample": s.describe() + "; one pass, each application's own timer",
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pm_oracle as O
+    if not O.ref_available():
+        raise RuntimeError("reference binaries not built (make -C oracle ref)")
+    off, idx = suite.A.csr()
+    ga = O.Graph(suite.A.n, off, idx)
+    f = O.write_binary(ga, os.path.join(O.tempdir(), "a"))
+    deg = np.diff(off)
+    per = {}
+    _, t = O.ref_components(f, threads=threads, result=False)
+    per["cc"] = (t, suite.A.m)
+    tb, eb = 0.0, 0
+    for s in suite.sources[:2]:
+        _, _, t = O.ref_bfs(f, s, threads=threads, parents=False)
+        tb += t
+        eb += int(deg[O.bfs(ga, s)[0] >= 0].sum())
+    per["bfs"] = (tb, eb)
+    secs = sum(v[0] for v in per.values())
+    edges = sum(v[1] for v in per.values())
+    return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS", "cores": threads, "kind": "reference",
+            "sample": "the reference programs (all host threads, their own timers) on graph A of the suite "
+                      "(symmetrised R-MAT scale %d): one Components run and BFS from the suite's first two "
+                      "sources" % int(np.log2(suite.A.n)),
             "per_algo": {k: round(v[1] / v[0] / 1e9, 5) for k, v in per.items()}}
 
 
 def run_reference(args):
+    """The reference arm: rank 0 alone runs the reference programs on the
+    suite's own graphs (RefSample); other ranks exit without work."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     threads = cpu_threads()
-    s = CpuSample(18, n_sources=2, wscale=17)
-    for _ in range(args.warmup):
-        s.step(threads)
-    tot_s, tot_e = 0.0, 0
-    per = {}
-    for _ in range(args.steps):
-        secs, edges, p = s.step(threads)
-        tot_s += secs
-        tot_e += edges
-        for k, v in p.items():
-            a = per.setdefault(k, [0.0, 0])
-            a[0] += v[0]
-            a[1] += v[1]
+    s = RefSample(args.scale_a, args.scale_b, args.sources)
+    tot_s, tot_e, per = s.run(args.warmup, args.steps, threads)
     value = tot_e / tot_s / 1e9
+    sample = s.describe(args.steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GTEPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * tot_s / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64/i32", "data": "synthetic",
-        "config": {"workload": "six-application suite, CPU sample: " + s.describe(),
-                   "threads": threads, "kind": s.kind},
-        "per_algo": {k: {"gteps": round(v[1] / v[0] / 1e9, 5), "ms": round(1000 * v[0] / args.steps, 3)}
+        "config": suite_config(args.scale_a, args.scale_b, args.sources, s.nA, s.mA, s.nB, s.mB, world),
+        "reference_sample": sample,
+        "per_algo": {k: {"gteps": round(v[1] / v[0] / 1e9, 5), "ms_per_step": round(1000 * v[0] / args.steps, 3)}
                      for k, v in per.items()},
-        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": threads, "kind": s.kind,
-                         "sample": s.describe()},
+        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": threads, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": round(value, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -847,7 +875,7 @@ def main():
     value = tot_edges_all / args.steps / (ms_step / 1e3) / 1e9
     hbm, peak_kind = peaks()
     nB, mB = suite.B.n, suite.B.m
-    pass_bytes = 8 * mB + 32 * nB
+    pass_bytes = 8 * mB + 16 * nB
     pass_ms = pr_ms / max(pr_passes, 1)
     achieved = pass_bytes / (pass_ms / 1e3) / 1e9 if pr_passes else None
     per_algo = {}
@@ -860,27 +888,22 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32",
         "data": "synthetic",
-        "config": {
-            "workload": "six-application suite: BFS x%d + CC + BellmanFord on symmetrised R-MAT "
-                        "scale %d ef16 (n=%d, m=%d); PageRank 20 it + SpMV 10 it + BP 10 it on "
-                        "directed R-MAT scale %d ef16 (n=%d, m=%d)"
-                        % (len(suite.sources), args.scale_a, suite.A.n, suite.A.m, args.scale_b,
-                           nB, mB),
-            "graphs": {"A": {"scale": args.scale_a, "n": suite.A.n, "m": suite.A.m},
-                       "B": {"scale": args.scale_b, "n": nB, "m": mB}},
-            "l2": "inputs larger than L2 (126 MB): graph A ids %d MB, graph B ids %d MB"
-                  % (suite.A.m * 4 >> 20, mB * 4 >> 20),
-            "parallelism": "replicas x%d" % world,
-            "launch": "direct launches (--no-cuda-graphs)" if args.no_cuda_graphs else
-                      "CUDA graphs: captured PageRank/SpMV/BP loops, device-driven BFS rounds",
-        },
+        "config": suite_config(args.scale_a, args.scale_b, len(suite.sources), suite.A.n, suite.A.m, nB, mB,
+                               world),
+        "launch": "direct launches (--no-cuda-graphs)" if args.no_cuda_graphs else
+                  "CUDA graphs: captured PageRank/SpMV/BP loops, device-driven BFS rounds",
         "per_algo": per_algo,
         "roofline": {
             "kernel": "PageRank pull-reduce pass (k_heavy_reduce + k_pull_reduce<PR_F<float>>)",
             "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
             "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / hbm, 4) if achieved else None,
-            "traffic": ncu_traffic(), "algorithmic_bytes_per_pass": pass_bytes,
+            "traffic": ncu_traffic(),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the pass, from the "
+                              "committed summary profiles/pagerank_pull_rmat24.md (not measured in this run)",
+            "algorithmic_bytes_per_pass": pass_bytes,
+            "algorithmic_bytes_rule": "8 m + 16 n: CSC id + gathered contribution per edge; offset, "
+                                      "out-degree, rank write, contribution write per vertex",
             "pass_ms": round(pass_ms, 4), "passes": pr_passes,
         },
         "gpu_launches": int(launches),
@@ -902,10 +925,10 @@ def main():
         pm.release_memory_cache()  # the blocks of its graphs
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_baseline(suite)
         except Exception as exc:  # keep the GPU line even if the CPU sample fails
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
-    line["errors_vs_fp64"] = errors_block(pm, suite)
+    line["errors_vs_gpu_fp64"] = errors_block(pm, suite)
     if not args.no_batched:
         line["batched"] = batched_block(pm, suite)
         line["adjoint"] = adjoint_block(pm, torch, suite.dev)
