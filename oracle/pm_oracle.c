@@ -702,6 +702,59 @@ PMO_API void pmo_bp(int64_t n, const int32_t *off, const int32_t *idx, const dou
 }
 
 /* ------------------------------------------------------------------------ */
+/* BP as the reference writes it, in linear products (FP64):                 */
+/* BP_F::updateAtomic (numa-BP.C:112-125) for each out-edge e = (s -> d) of   */
+/* a frontier source s, sources ascending: belief_e[i] = sum_j prior_d[j] *  */
+/* psi[i][j] * prod_curr_d[j]; prod_next_d[i] *= belief_e[i]; d joins the    */
+/* next frontier.  BP_Vertex_Reset (130-140) sets prod_next = 1 on the       */
+/* current frontier first; the arrays swap every round (loop 280-316).       */
+/* Products start at 1 in prod_curr and 0 in prod_next (the zero-filled      */
+/* mapping), every vertex in the first frontier.  normalize != 0 divides     */
+/* each belief by its sum before the product (the messages pmo_bp uses, in   */
+/* the linear domain).  psi: 4 doubles [i][j] for every edge.  out: n x 2.   */
+/* ------------------------------------------------------------------------ */
+PMO_API void pmo_bp_raw(int64_t n, const int32_t *off, const int32_t *idx, const double *prior,
+                        const double *psi, int iters, int normalize, double *out_prod) {
+  double *Pc = (double *)malloc((size_t)n * 2 * sizeof(double));
+  double *Pn = (double *)malloc((size_t)n * 2 * sizeof(double));
+  unsigned char *F = (unsigned char *)malloc((size_t)n);
+  unsigned char *Nx = (unsigned char *)malloc((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    Pc[2 * i] = Pc[2 * i + 1] = 1.0;
+    Pn[2 * i] = Pn[2 * i + 1] = 0.0;
+    F[i] = 1;
+  }
+  for (int it = 0; it < iters; ++it) {
+    memset(Nx, 0, (size_t)n);
+    for (int64_t i = 0; i < n; ++i)
+      if (F[i]) { Pn[2 * i] = 1.0; Pn[2 * i + 1] = 1.0; }
+    for (int64_t s = 0; s < n; ++s) {
+      if (!F[s]) continue;
+      for (int64_t e = off[s]; e < off[s + 1]; ++e) {
+        int32_t d = idx[e];
+        double b[2];
+        for (int i = 0; i < 2; ++i) {
+          b[i] = 0.0;
+          for (int j = 0; j < 2; ++j) b[i] += prior[2 * d + j] * psi[2 * i + j] * Pc[2 * d + j];
+        }
+        if (normalize) {
+          double z = b[0] + b[1];
+          b[0] /= z;
+          b[1] /= z;
+        }
+        Pn[2 * d] *= b[0];
+        Pn[2 * d + 1] *= b[1];
+        Nx[d] = 1;
+      }
+    }
+    double *t = Pc; Pc = Pn; Pn = t;
+    unsigned char *tb = F; F = Nx; Nx = tb;
+  }
+  memcpy(out_prod, Pc, (size_t)n * 2 * sizeof(double));
+  free(Pc); free(Pn); free(F); free(Nx);
+}
+
+/* ------------------------------------------------------------------------ */
 /* PBBS writers read by the reference loaders (IO-numa.h / IO.h):            */
 /*  AdjacencyGraph text (IO-numa.h:112-188), WeightedAdjacencyGraph text     */
 /*  (IO-numa.h:318-402: offsets, then destinations, then weights) and the    */

@@ -88,6 +88,7 @@ def lib():
             "pmo_bellman_ford": (C.c_int, [i64, i32p, i32p, i32p, i32, i32p]),
             "pmo_dijkstra": (None, [i64, i32p, i32p, i32p, i32, i32p]),
             "pmo_bp": (None, [i64, i32p, i32p, f64p, C.c_void_p, f64p, C.c_int, f64p]),
+            "pmo_bp_raw": (None, [i64, i32p, i32p, f64p, f64p, C.c_int, C.c_int, f64p]),
             "pmo_write_adj_text": (C.c_int, [C.c_char_p, i64, i32p, i32p, C.c_void_p]),
             "pmo_write_adj_binary": (C.c_int, [C.c_char_p, i64, i32p, i32p]),
         }
@@ -318,6 +319,24 @@ def bp(g: Graph, prior, iters: int, psi_uniform=None, psi_edge=None) -> np.ndarr
     return out.reshape(g.n, 2)
 
 
+def bp_raw(g: Graph, prior, iters: int, normalize: bool = False, psi=((0.9, 0.1), (0.1, 0.9))) -> np.ndarray:
+    """Linear products (n x 2) of BP as the reference writes it (pmo_bp_raw):
+    unnormalised beliefs, or with normalize each belief divided by its sum."""
+    out = np.empty(2 * g.n, np.float64)
+    lib().pmo_bp_raw(g.n, g.off, _idx(g), np.ascontiguousarray(prior, np.float64).reshape(-1),
+                     np.ascontiguousarray(psi, np.float64).reshape(4), iters, int(normalize), out)
+    return out.reshape(g.n, 2)
+
+
+def bp_ref_priors(n: int) -> np.ndarray:
+    """The priors the patched reference BP sets (ref_patch_bp.py), as float32:
+    p0 = (float)(0.2 + 0.6 * ((37 v + 11) mod 101) / 101), p1 = 1 - p0."""
+    v = np.arange(n, dtype=np.int64)
+    p0 = (0.2 + 0.6 * ((37 * v + 11) % 101).astype(np.float64) / 101.0).astype(np.float32)
+    p1 = np.float32(1.0) - p0
+    return np.stack([p0, p1], axis=1)
+
+
 def bfs_depths_from_parents(parents: np.ndarray, src: int) -> np.ndarray:
     """Depth of every vertex by walking the parent array (-1: unreached).
     Raises ValueError on a cycle or a parent chain that misses src."""
@@ -453,6 +472,20 @@ def ref_pagerank(path: str, iters: int, binary: bool = True, threads=None, resul
     r = np.zeros(len(vals), np.float64)
     for i, v in vals:
         r[int(i)] = float(v)
+    return r, t
+
+
+def ref_bp_result(path: str, iters: int, binary: bool = True, timeout=600):
+    """numa-BP-result <g> <iters> -result -a [-b] on one thread (the
+    reference multiplies products without atomics); returns (n x 2 products,
+    seconds)."""
+    args = [os.path.join(REF_DIR, "numa-BP-result"), path, str(iters), "-result", "-a",
+            "-b" if binary else "-t"]
+    out, t = _run(args, 1, timeout)
+    vals = re.findall(r"^prod (\d+) ([0-9.eE+-]+) ([0-9.eE+-]+)$", out, re.M)
+    r = np.zeros((len(vals), 2), np.float64)
+    for i, a, b in vals:
+        r[int(i)] = (float(a), float(b))
     return r, t
 
 

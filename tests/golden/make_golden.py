@@ -6,7 +6,8 @@ stores their outputs, together with the graphs, as .npz files.  The fixtures
 pin the CPU oracle (oracle/pm_oracle.c) on machines without the reference
 and pin the synthetic-graph generator itself.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py bp       # the BP fixture only
 """
 from __future__ import annotations
 
@@ -37,11 +38,34 @@ def tiny_graph():
     return n, off, idx, src, dst
 
 
+def bp_graph():
+    """A sparse seeded directed graph (in-degree at most 10), where two rounds
+    of the reference's unnormalised FP32 products stay in the normal range."""
+    rng = np.random.default_rng(7)
+    n, m = 3000, 9000
+    return O.graph_from_edges(n, rng.integers(0, n, m), rng.integers(0, n, m))
+
+
+def bp_fixture(d):
+    """numa-BP with its inputs set and its products printed (numa-BP-result,
+    oracle/ref_patch_bp.py), one thread, after 1 and 2 rounds."""
+    g = bp_graph()
+    base = O.write_binary(g, os.path.join(d, "bp"))
+    p1, _ = O.ref_bp_result(base, 1)
+    p2, _ = O.ref_bp_result(base, 2)
+    np.savez_compressed(os.path.join(HERE, "bp_sparse.npz"), off=g.off, idx=g.idx, prod1=p1, prod2=p2)
+    return g.n, g.m
+
+
 def main():
     if not O.ref_available():
         O.build()
     d = O.tempdir()
     out = {}
+    if sys.argv[1:] == ["bp"]:
+        print("bp_sparse          n=%d m=%d" % bp_fixture(d))
+        return
+    out["bp_sparse"] = bp_fixture(d)
 
     # --- directed scale-10 R-MAT: PageRank, SpMV ---------------------------
     g = O.rmat_graph(10, 16)

@@ -594,3 +594,21 @@ def test_kernel_launch_counter(pm):
         pm.kernel_launches(reset=True)
         pm.PageRank(g, 5, dtype=np.float32)
         assert pm.kernel_launches() >= 5
+
+
+def test_bp_on_reference_pinned_inputs(pm, oracle):
+    """The graph and priors the patched reference BP was run on
+    (tests/golden/bp_sparse.npz): the GPU's FP64 log-products equal the log of
+    the reference formula with each message divided by its sum
+    (pmo_bp_raw normalize), whose unnormalised form the fixture pins to the
+    reference's own output."""
+    z = load("bp_sparse.npz")
+    og = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    prior = oracle.bp_ref_priors(og.n)
+    with dev_graph(pm, og) as g:
+        for it in (1, 2, 4):
+            lp = pm.BeliefPropagation(g, prior.astype(np.float64), it, dtype=np.float64)
+            want = oracle.bp_raw(og, prior.astype(np.float64), it, normalize=True)
+            assert np.allclose(np.exp(lp), want, rtol=1e-9, atol=0), it
+            lp32 = pm.BeliefPropagation(g, prior, it)
+            assert rel_l1(lp32, np.log(want)) < RL1_F32, it

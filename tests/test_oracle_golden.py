@@ -136,6 +136,49 @@ def test_bp_restatement_small(oracle):
     assert np.allclose(out[0], [0, 0])
 
 
+# The reference's BP prints nothing and leaves its inputs unset; a patched
+# copy (oracle/ref_patch_bp.py: seeded priors, products 1, psi
+# [[.9,.1],[.1,.9]], products printed) pins the message formula.  Its FP32
+# arithmetic against the FP64 restatement: relative 2e-5 over two rounds.
+RTOL_BP_FP32 = 2e-5
+
+
+def test_bp_raw_matches_reference_fixture(oracle):
+    z = np.load(os.path.join(GOLDEN, "bp_sparse.npz"))
+    g = oracle.Graph(len(z["off"]) - 1, z["off"], z["idx"])
+    prior = oracle.bp_ref_priors(g.n).astype(np.float64)
+    for it, key in ((1, "prod1"), (2, "prod2")):
+        raw = oracle.bp_raw(g, prior, it)
+        assert np.allclose(z[key], raw, rtol=RTOL_BP_FP32, atol=0), it
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
+                                                    "numa-BP-result")), reason="reference binaries not built")
+def test_bp_raw_matches_live_reference(oracle, tmp_path):
+    rng = np.random.default_rng(11)
+    n, m = 2000, 5000
+    g = oracle.graph_from_edges(n, rng.integers(0, n, m), rng.integers(0, n, m))
+    base = oracle.write_binary(g, str(tmp_path / "bp"))
+    prior = oracle.bp_ref_priors(n).astype(np.float64)
+    for it in (1, 2):
+        ref, _ = oracle.ref_bp_result(base, it)
+        assert np.allclose(ref, oracle.bp_raw(g, prior, it), rtol=RTOL_BP_FP32, atol=0), it
+
+
+def test_bp_log_restatement_is_the_normalised_formula(oracle):
+    """pmo_bp (log products of messages divided by their sum) equals the
+    reference's formula with each belief divided by its sum, in the linear
+    domain: the only change from the reference's messages is that division."""
+    rng = np.random.default_rng(3)
+    for n, m in ((500, 1500), (4000, 20000)):
+        g = oracle.graph_from_edges(n, rng.integers(0, n, m), rng.integers(0, n, m))
+        prior = oracle.uniform_open(2 * n, 99).reshape(n, 2).astype(np.float64)
+        for it in (1, 2, 4):
+            a = np.exp(oracle.bp(g, prior, it))
+            b = oracle.bp_raw(g, prior, it, normalize=True)
+            assert np.allclose(a, b, rtol=1e-12, atol=0), (n, it)
+
+
 def test_er_batch_generator(oracle):
     g, vbase = oracle.er_batch(40, 50, 5000, 8, seed=3)
     sizes = np.diff(vbase)
