@@ -1305,6 +1305,8 @@ struct Tunables {
                                      // 1 push over the frontier's out-edges (DENSE_FORWARD)
   int32_t cc_mode = 0;               // Components on a symmetric graph: 0 union-find,
                                      // 1 label propagation (the reference's rounds)
+  int32_t bf_delta = 0;              // BellmanFord: > 0 relaxes only frontier vertices below a
+                                     // bound that moves by this much (delta-stepping); 0 all
 };
 
 // Key of a captured loop: its name and every value its launches bake in.

@@ -466,6 +466,12 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       (threshold chooses their direction).  Same labels
                                       either way; directed and partition handles always
                                       propagate */
+#define PM_TUNE_BF_DELTA 13        /* BellmanFord schedule: 0 (default) every round
+                                      relaxes the whole frontier; Delta > 0 relaxes only
+                                      the frontier vertices with dist < T, the others wait,
+                                      and T moves to (least waiting distance) + Delta when
+                                      none is below it (delta-stepping).  Same distances;
+                                      range [0, 2^30]; ignored on a partition handle */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

@@ -377,6 +377,132 @@ __global__ void k_bf_init(int32_t *dist, int64_t n, int32_t src) {
     dist[v] = v == src ? 0 : kDevBFInf;
 }
 
+// Delta-stepping schedule (tunable bf_delta = Delta > 0).  The frontier F
+// holds the vertices whose distance fell and whose out-edges are not yet
+// relaxed.  Each round relaxes only F_near = {v in F : dist[v] < T}; the
+// others stay in F for a later round.  When F_near is empty, T moves to the
+// least distance left in F plus Delta.  Any order of relaxing the vertices
+// whose distance fell ends at the exact shortest distances, so the result
+// is the plain rounds' result; relaxing near vertices first lets fewer
+// distances fall twice.
+__global__ void k_bf_split(int32_t n, const int32_t *__restrict__ out_off, const uint32_t *__restrict__ cur,
+                           const int32_t *dist, int32_t T, uint32_t *__restrict__ near, uint32_t *__restrict__ far,
+                           Counters *c) {
+  const int64_t words = ((int64_t)n + 31) / 32;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long ns = 0, ne = 0, fs = 0, far_top = 0;  // far_top: max of (kDevBFInf - dist)
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) {
+    uint32_t w = cur[i], wn = 0, wf = 0;
+    while (w) {
+      const int b = __ffs(w) - 1;
+      w &= w - 1;
+      const int v = (int)(i * 32 + b);
+      const int32_t d = *((volatile const int32_t *)dist + v);
+      if (d < T) {
+        wn |= 1u << b;
+        ns++;
+        ne += __ldg(out_off + v + 1) - __ldg(out_off + v);
+      } else {
+        wf |= 1u << b;
+        fs++;
+        far_top = max(far_top, (unsigned long long)(kDevBFInf - min(d, kDevBFInf)));
+      }
+    }
+    near[i] = wn;
+    far[i] = wf;
+  }
+  ns = warp_sum(ns);
+  ne = warp_sum(ne);
+  fs = warp_sum(fs);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) far_top = max(far_top, __shfl_down_sync(0xffffffffu, far_top, d));
+  if (lane_id() == 0) {
+    if (ns) {
+      atomicAdd(&c[0].size, ns);
+      atomicAdd(&c[0].edges, ne);
+    }
+    if (fs) {
+      atomicAdd(&c[1].size, fs);
+      atomicMax(&c[1].aux, far_top);
+    }
+  }
+}
+
+// dst |= src, counting the union's size and out-degree sum.
+__global__ void k_bits_or_count(int32_t n, const int32_t *__restrict__ out_off, uint32_t *dst,
+                                const uint32_t *__restrict__ src, Counters *c) {
+  const int64_t words = ((int64_t)n + 31) / 32;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long s = 0, e = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) {
+    uint32_t w = dst[i] | src[i];
+    dst[i] = w;
+    s += __popc(w);
+    while (w) {
+      const int b = __ffs(w) - 1;
+      w &= w - 1;
+      const int v = (int)(i * 32 + b);
+      e += __ldg(out_off + v + 1) - __ldg(out_off + v);
+    }
+  }
+  s = warp_sum(s);
+  e = warp_sum(e);
+  if (lane_id() == 0 && s) {
+    atomicAdd(&c->size, s);
+    atomicAdd(&c->edges, e);
+  }
+}
+
+static void run_bellman_ford_delta(pm_graph *g, int32_t *d_dist, int64_t threshold, bool push, VertexSubset &cur,
+                                   VertexSubset &next, pm_traversal_stats &s) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  const int32_t delta = E.tune.bf_delta;
+  const int32_t *w_out = g->w_i32_out.as<int32_t>(), *w_in = g->w_i32_in.as<int32_t>();
+  VertexSubset near;
+  near.n = (int32_t)n;
+  near.bits = (uint32_t *)g->scratch_buf(33, (size_t)cur.words() * 4);
+  near.queue = (int32_t *)g->scratch_buf(34, (size_t)n * 4);
+  uint32_t *far = (uint32_t *)g->scratch_buf(35, (size_t)cur.words() * 4);
+  Counters *dc = (Counters *)g->scratch_buf(32, 2 * sizeof(Counters));
+  Counters hc[2];
+  const int grid = E.grid_for(cur.words(), 256, 16);
+  int64_t T = delta;
+  while (cur.size > 0) {
+    PM_CUDA(cudaMemsetAsync(dc, 0, 2 * sizeof(Counters), E.stream));
+    PM_LAUNCH(k_bf_split, grid, 256, 0, E.stream, (int32_t)n, E.g.out.off, cur.bits, d_dist,
+              (int32_t)std::min<int64_t>(T, kDevBFInf), near.bits, far, dc);
+    PM_CUDA(cudaMemcpyAsync(hc, dc, 2 * sizeof(Counters), cudaMemcpyDeviceToHost, E.stream));
+    PM_CUDA(cudaStreamSynchronize(E.stream));
+    near.size = (int64_t)hc[0].size;
+    near.edges = (int64_t)hc[0].edges;
+    near.has_queue = false;
+    if (near.size == 0) {  // the rest lies at T or beyond: next bound from the least of it
+      const int64_t least = (int64_t)kDevBFInf - (int64_t)hc[1].aux;
+      T = std::max<int64_t>(T, least) + delta;
+      continue;
+    }
+    bool dense = false;
+    s.edges_visited += near.edges;
+    if (push)
+      edgeMap<int32_t>(E, near, BF_F{d_dist, near.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, &dense);
+    else
+      edgeMapReduce<int32_t>(E, near, BF_F{d_dist, near.bits}, next, threshold, w_out, w_in, &dense);
+    // the new frontier: what fell this round and what waited
+    PM_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), E.stream));
+    PM_LAUNCH(k_bits_or_count, grid, 256, 0, E.stream, (int32_t)n, E.g.out.off, next.bits, far, dc);
+    PM_CUDA(cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, E.stream));
+    PM_CUDA(cudaStreamSynchronize(E.stream));
+    next.size = (int64_t)hc[0].size;
+    next.edges = (int64_t)hc[0].edges;
+    next.has_queue = false;
+    s.rounds++;
+    s.dense_rounds += dense;
+    std::swap(cur, next);
+    if (s.rounds > 4 * (g->n + 1)) fail(PM_ERR_INVALID_ARG, "BellmanFord did not converge");
+  }
+}
+
 void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t threshold,
                       pm_traversal_stats *st) {
   Engine &E = g->E;
@@ -390,6 +516,11 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
   // dense rounds: the pull-reduce, or the reference's dense push (DENSE_FORWARD,
   // numa-BellmanFord.C:182), which reads only the frontier's out-edges
   const bool push = E.tune.bf_dense == 1 && !g->is_part;
+  if (E.tune.bf_delta > 0 && !g->is_part) {
+    run_bellman_ford_delta(g, d_dist, threshold, push, cur, next, s);
+    if (st) *st = s;
+    return;
+  }
   while (cur.size > 0) {
     bool dense = false;
     s.edges_visited += cur.edges;

@@ -43,6 +43,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_MULTI_DIV: return t.multi_div;
     case PM_TUNE_BF_DENSE: return t.bf_dense;
     case PM_TUNE_CC_MODE: return t.cc_mode;
+    case PM_TUNE_BF_DELTA: return t.bf_delta;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -93,6 +94,9 @@ void check_tunable(int key, int64_t value) {
       break;
     case PM_TUNE_CC_MODE:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cc_mode must be 0 or 1");
+      break;
+    case PM_TUNE_BF_DELTA:
+      if (value < 0 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "bf_delta must be in [0, 2^30]");
       break;
     case PM_TUNE_HEAVY_MODE:
       if (value < 0 || value > 2) fail(PM_ERR_INVALID_ARG, "heavy_mode must be 0, 1 or 2");
@@ -191,7 +195,7 @@ static void add_app(pm_graph *g, int app, std::vector<std::function<void()>> &ru
       const int32_t src = tune_sources(g, 1)[0];
       int32_t *d = (int32_t *)slot(8, (size_t)n * 4);
       runs.push_back([=] { run_bellman_ford(g, src, d, g->m / g->E.tune.bf_div, nullptr); });
-      add_keys({PM_TUNE_BF_DENSE, PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND,
+      add_keys({PM_TUNE_BF_DELTA, PM_TUNE_BF_DENSE, PM_TUNE_BF_DIV, PM_TUNE_CTA_EXPAND, PM_TUNE_GRID_EXPAND,
                 PM_TUNE_HEAVY_DEG, PM_TUNE_HEAVY_MODE, PM_TUNE_PULL_CTAS_PER_SM});
       break;
     }
@@ -249,6 +253,7 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
         case PM_TUNE_GRID_EXPAND: cands = {128, 256, 512, 1024, 4096}; break;
         case PM_TUNE_HEAVY_MODE: cands = {0, 1, 2}; break;
         case PM_TUNE_BF_DENSE: cands = {0, 1}; break;
+        case PM_TUNE_BF_DELTA: cands = {0, 4, 8, 16, 32}; break;
         case PM_TUNE_PULL_CTAS_PER_SM:
           cands.push_back(0);
           for (int c = 1; c < occupancy; ++c) cands.push_back(c);

@@ -315,6 +315,30 @@ def test_bellman_ford_dense_push_exact(pm, oracle, threshold):
                         assert st["dense_rounds"] == st["rounds"]
 
 
+@pytest.mark.parametrize("bf_dense", [0, 1])
+@pytest.mark.parametrize("delta", [1, 4, 16, 1 << 20])
+def test_bellman_ford_delta_stepping_exact(pm, oracle, delta, bf_dense):
+    """The delta-stepping schedule (bf_delta): only frontier vertices below a
+    moving bound relax each round; distances equal Dijkstra's in every
+    direction regime, dense rounds pulled or pushed, on both graph kinds and
+    on a hub graph; a huge Delta is the plain schedule."""
+    n = 12288
+    src = np.concatenate([np.arange(1, n), np.zeros(n - 1, np.int64), np.arange(1, n - 1)])
+    dst = np.concatenate([np.zeros(n - 1, np.int64), np.arange(1, n), np.arange(2, n)])
+    hub = oracle.graph_from_edges(n, src, dst)
+    for og, sym in ((oracle.rmat_graph(13, 16, symmetric=True), True), (oracle.rmat_graph(13, 16), False),
+                    (hub, False)):
+        w = oracle.weights_int(og)
+        with dev_graph(pm, og, symmetric=sym) as g:
+            g.set_weights(w)
+            g.set_tunable("bf_delta", delta)
+            g.set_tunable("bf_dense", bf_dense)
+            for s in [int(v) for v in oracle.pick_sources(og, 2)]:
+                want = oracle.dijkstra(og, w, s)
+                for thr in (-1, 0, 1 << 40):
+                    assert np.array_equal(pm.BellmanFord(g, s, threshold=thr), want), (delta, thr, s)
+
+
 def test_bellman_ford_dense_push_hub(pm, oracle):
     """A hub of in- and out-degree 12287 on a ring (three heavy chunks per
     direction, a ragged last chunk): every round dense, pushed."""
