@@ -371,6 +371,59 @@ struct BF_F {
   }
 };
 
+// Dense pulls read a snapshot taken at the start of the round: fd[s] =
+// dist[s] for frontier sources, INT_MAX for the others, so that an edge costs
+// one gather (BF_F's bit test and then the distance are two dependent loads;
+// the pull was latency-bound on them).  Relaxing from the round's snapshot
+// is the synchronous form of the same rounds and reaches the same fixpoint.
+struct BF_FD {
+  int32_t *dist;
+  const int32_t *fd;
+  using Acc = int32_t;
+  __device__ __forceinline__ bool cond(int) const { return true; }
+  __device__ __forceinline__ bool updateAtomic(int s, int d, int32_t w) const {
+    int32_t nd = *((volatile int32_t *)dist + s) + w;
+    return nd < atomicMin(dist + d, nd);
+  }
+  __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
+  __device__ __forceinline__ Acc edge(int s, int, int32_t w) const {
+    const int32_t v = __ldg(fd + s);
+    return v == 0x7fffffff ? v : v + w;
+  }
+  __device__ __forceinline__ Acc combine(Acc a, Acc b) const { return min(a, b); }
+  __device__ __forceinline__ bool commit(int d, Acc acc, double2 &) const {
+    if (acc < dist[d]) {
+      dist[d] = acc;
+      return true;
+    }
+    return false;
+  }
+};
+
+__global__ void k_bf_snapshot(int32_t n, const uint32_t *__restrict__ bits, const int32_t *__restrict__ dist,
+                              int32_t *__restrict__ fd) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+    fd[v] = test_bit(bits, (int)v) ? dist[v] : 0x7fffffff;
+}
+
+// One BellmanFord round from `from` into `next`: the reference's dense push
+// (DENSE_FORWARD) when push, else the pull-reduce, which for a dense round
+// reads the frontier's distances from a snapshot.
+static void bf_round(pm_graph *g, VertexSubset &from, VertexSubset &next, int64_t threshold, bool push,
+                     int32_t *d_dist, const int32_t *w_out, const int32_t *w_in, bool *dense) {
+  Engine &E = g->E;
+  if (push) {
+    edgeMap<int32_t>(E, from, BF_F{d_dist, from.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, dense);
+  } else if (go_dense(from, threshold) && !g->is_part) {
+    int32_t *fd = (int32_t *)g->scratch_buf(36, (size_t)g->n * 4);
+    PM_LAUNCH(k_bf_snapshot, E.grid_for(g->n, 256, 16), 256, 0, E.stream, (int32_t)g->n, from.bits, d_dist, fd);
+    edgeMapReduce<int32_t>(E, from, BF_FD{d_dist, fd}, next, threshold, w_out, w_in, dense);
+  } else {
+    edgeMapReduce<int32_t>(E, from, BF_F{d_dist, from.bits}, next, threshold, w_out, w_in, dense);
+  }
+}
+
 __global__ void k_bf_init(int32_t *dist, int64_t n, int32_t src) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
@@ -484,10 +537,7 @@ static void run_bellman_ford_delta(pm_graph *g, int32_t *d_dist, int64_t thresho
     }
     bool dense = false;
     s.edges_visited += near.edges;
-    if (push)
-      edgeMap<int32_t>(E, near, BF_F{d_dist, near.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, &dense);
-    else
-      edgeMapReduce<int32_t>(E, near, BF_F{d_dist, near.bits}, next, threshold, w_out, w_in, &dense);
+    bf_round(g, near, next, threshold, push, d_dist, w_out, w_in, &dense);
     // the new frontier: what fell this round and what waited
     PM_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), E.stream));
     PM_LAUNCH(k_bits_or_count, grid, 256, 0, E.stream, (int32_t)n, E.g.out.off, next.bits, far, dc);
@@ -524,10 +574,7 @@ void run_bellman_ford(pm_graph *g, int32_t src, int32_t *d_dist, int64_t thresho
   while (cur.size > 0) {
     bool dense = false;
     s.edges_visited += cur.edges;
-    if (push)
-      edgeMap<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, &dense);
-    else
-      edgeMapReduce<int32_t>(E, cur, BF_F{d_dist, cur.bits}, next, threshold, w_out, w_in, &dense);
+    bf_round(g, cur, next, threshold, push, d_dist, w_out, w_in, &dense);
     part_exchange(g, d_dist, 4);  // a partition: distances and frontier of every rank
     part_round(g, next);
     s.rounds++;
