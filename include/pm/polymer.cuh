@@ -535,6 +535,54 @@ constexpr int kPullBlock = PM_PULL_BLOCK;
 constexpr int kHubBlock = 768;
 constexpr int kHubMax = 16384;
 
+#ifndef PM_STAGE_IDS
+#define PM_STAGE_IDS 512
+#endif
+// Staged pull (k_pull_reduce with STAGE): the CSC ids of a warp's batch of 32
+// rows, when they are at most kStageIds, are copied into the warp's slice of
+// shared memory by one bulk copy (cp.async.bulk global -> shared, completed
+// on an mbarrier) and read from there.  The id loads then cost no L1 tag
+// look-ups, which the gathers of the same SM are bound by, and a window
+// waits for one copy per batch instead of its own id loads.  The copy's
+// source starts at the 16-byte boundary below the batch's first id and its
+// size is rounded up to 16 bytes (never past the last aligned id of the
+// array: a batch ending beyond it reads from global memory).
+constexpr int kStageIds = PM_STAGE_IDS;
+constexpr int kStageWaitTries = 1 << 20;  // polls of a copy's mbarrier before giving up
+// dynamic shared memory of a staged kPullBlock CTA: the warps' mbarriers in
+// the first 128 bytes, then each warp's kStageIds ids
+constexpr size_t kStageSmem = 128 + (size_t)(kPullBlock / 32) * kStageIds * 4;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bytes: a multiple of 16; src and dst 16-byte aligned; src in this GPU's memory
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// orders this thread's earlier generic accesses to shared memory before
+// later asynchronous (bulk copy) writes to it
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // Sources whose values a pull keeps in shared memory: idx is the CSC source
 // array with the cached sources' slots stored as ~slot, vals their values
 // for this pass.
@@ -688,10 +736,12 @@ __device__ __forceinline__ bool wait_at_least(const int32_t *p, int32_t target, 
 // cached sources appear as ~slot and their values are read from shared
 // memory (loaded from hubs.vals once per CTA); two kHubBlock-thread CTAs per
 // SM.  The values are the ones edge() would load, so results are unchanged.
-template <class F, class W, int MODE = 0, bool HUBS = false>
+template <class F, class W, int MODE = 0, bool HUBS = false, bool STAGE = false>
 __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_PULL_MINB)
     k_pull_reduce(GraphView g, F f, const W *__restrict__ w, typename F::Acc *partials, int32_t *hdone,
                   uint32_t *__restrict__ next, Counters *cnt, HubCache<typename F::Acc> hubs = {}) {
+  static_assert(!STAGE || (MODE == 0 && !HUBS && std::is_same<W, int>::value),
+                "staged ids: heavy mode 0, ids without paired weights, no hub cache");
   using Acc = typename F::Acc;
   constexpr int K = LaneEdgesTrait<F>::value, WIN = 32 * K, NW = (HUBS ? kHubBlock : kPullBlock) / 32;
   __shared__ Acc s_acc[NW][32];
@@ -709,6 +759,19 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
   Acc *acc_s = s_acc[wid];
   int *pos_s = s_pos[wid];
   int *off_s = s_off[wid];
+  // STAGE: [NW mbarriers][pad to 128 B][NW x kStageIds ids]
+  uint64_t *st_bar = reinterpret_cast<uint64_t *>(s_dyn) + wid;
+  int32_t *st_ids = reinterpret_cast<int32_t *>(s_dyn + 128) + (size_t)wid * kStageIds;
+  // bit 0: the mbarrier's phase; bit 1: a copy did not complete in time, the
+  // warp reads its ids from global memory from then on
+  uint32_t st_state = 0;
+  if constexpr (STAGE) {
+    if (lane == 0) {
+      mbar_init(st_bar, 1);
+      mbar_init_fence();
+    }
+    __syncwarp();
+  }
   unsigned long long my_size = 0, my_edges = 0;
   double2 my_aux = make_double2(0.0, 0.0);
   // persistent warps: each takes the next group from a ticket counter
@@ -737,12 +800,56 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
     }
     const bool heavy = deg > g.heavy_deg;
     const int ldeg = (live && !heavy) ? deg : 0;
+    // STAGE: the batch's CSC ids into this warp's shared slice
+    int st_base = 0;
+    bool staged = false;
+    if constexpr (STAGE) {
+      // ids are int here (m < 2^31); the copy is [a, b), 16-byte aligned,
+      // and ends at or before the last aligned id of the array
+      const int last = min(31, r_end - rb - 1);
+      const int first_e = __shfl_sync(0xffffffffu, o0, 0);
+      const int end_e = __shfl_sync(0xffffffffu, o0 + deg, last);
+      const int a = first_e & ~3, b = (int)(((int64_t)end_e + 3) & ~3ll);
+      staged = !(st_state & 2u) && end_e > first_e && b - a <= kStageIds && (int64_t)b <= (g.m & ~3ll);
+      if (staged) {
+        // every lane is done with the previous batch's ids (the __syncwarp
+        // that ends a batch); the copy runs while the batch is laid out
+        if (lane == 0) {
+          fence_proxy_async_smem();
+          mbar_expect_tx(st_bar, (uint32_t)((b - a) * 4));
+          bulk_copy_g2s(st_ids, g.in.idx + a, (uint32_t)((b - a) * 4), st_bar);
+        }
+        st_base = a;
+      }
+    }
     int total;
     const int pos = warp_excl_scan(ldeg, &total);
     pos_s[lane] = pos;
     if (lane == 31) pos_s[32] = total;
     off_s[lane] = o0;
     acc_s[lane] = f.identity();
+    if constexpr (STAGE) {
+      if (staged) {
+        // lane 0 waits for the copy (bounded), the warp learns the outcome
+        int done = 0;
+        if (lane == 0) {
+          for (int i = 0; i < kStageWaitTries && !done; ++i) done = mbar_try_wait(st_bar, st_state & 1u);
+          if (!done) {
+            // not complete in time: report it, wait once more (bounded) for
+            // the copy in flight, and read this and later batches from
+            // global memory
+            atomicOr(&cnt->err, (unsigned)kErrTimeout);
+            for (int i = 0; i < kStageWaitTries && !done; ++i) done = mbar_try_wait(st_bar, st_state & 1u);
+            done = 0;
+          }
+        }
+        if (!__shfl_sync(0xffffffffu, done, 0)) {
+          staged = false;
+          st_state |= 2u;
+        }
+        st_state ^= 1u;
+      }
+    }
     __syncwarp();
     for (int c = 0; c < total; c += WIN) {
       const int q0 = c + lane * K;
@@ -771,7 +878,9 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
 #pragma unroll
         for (int k = 0; k < K; ++k)
           src[k] = (32 * k + lane < cnt)
-                       ? checked_src<HUBS>(g, hubs.count, load_src(lidx, w, (int64_t)e0 + 32 * k + lane, wv[k]))
+                       ? checked_src<HUBS>(g, hubs.count,
+                                           (STAGE && staged) ? st_ids[e0 + 32 * k + lane - st_base]
+                                                             : load_src(lidx, w, (int64_t)e0 + 32 * k + lane, wv[k]))
                        : 0;
 #pragma unroll
         for (int k = 0; k < K; ++k)
@@ -804,7 +913,10 @@ __global__ void __launch_bounds__(HUBS ? kHubBlock : kPullBlock, HUBS ? 2 : PM_P
       typename EdgeT<W>::type wv[K];
 #pragma unroll
       for (int k = 0; k < K; ++k)
-        src[k] = (q0 + k < total) ? checked_src<HUBS>(g, hubs.count, load_src(lidx, w, es[k], wv[k])) : 0;
+        src[k] = (q0 + k < total)
+                     ? checked_src<HUBS>(g, hubs.count,
+                                         (STAGE && staged) ? st_ids[es[k] - st_base] : load_src(lidx, w, es[k], wv[k]))
+                     : 0;
       Acc vals[K];
 #pragma unroll
       for (int k = 0; k < K; ++k)
@@ -1307,6 +1419,8 @@ struct Tunables {
                                      // 1 label propagation (the reference's rounds)
   int32_t bf_delta = 0;              // BellmanFord: > 0 relaxes only frontier vertices below a
                                      // bound that moves by this much (delta-stepping); 0 all
+  int32_t pull_stage = 0;            // pull-reduce: 1 copies each batch's CSC ids to shared
+                                     // memory with one bulk copy (unweighted / int weights)
 };
 
 // Key of a captured loop: its name and every value its launches bake in.
@@ -1595,6 +1709,21 @@ void launch_pull_reduce(Engine &E, F f, const W *w_in, uint32_t *next_bits, Coun
     PM_LAUNCH((k_heavy_commit<F>), E.grid_for(E.g.in.nchunks, 256, 4), 256, 0, E.stream, E.g, f,
               (const Acc *)partials, next_bits, cnt);
   } else {
+    if constexpr (std::is_same<W, int>::value) {
+      // staged ids: the bulk copies need a 16-byte aligned id array
+      if (E.tune.pull_stage && ((uintptr_t)E.g.in.idx & 15) == 0) {
+        constexpr size_t smem = kStageSmem;
+        static const int stage_per_sm = [] {
+          int r = 0;
+          PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_pull_reduce<F, W, 0, false, true>,
+                                                                kPullBlock, smem));
+          return std::max(r, 1);
+        }();
+        PM_LAUNCH((k_pull_reduce<F, W, 0, false, true>), E.persistent_grid(want, stage_per_sm), kPullBlock, smem,
+                  E.stream, E.g, f, w_in, partials, (int32_t *)nullptr, next_bits, cnt, HubCache<Acc>{});
+        return;
+      }
+    }
     PM_LAUNCH((k_pull_reduce<F, W, 0>), E.persistent_grid(want, per_sm[0]), kPullBlock, 0, E.stream, E.g, f,
               w_in, partials, (int32_t *)nullptr, next_bits, cnt);
   }

@@ -472,6 +472,11 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       and T moves to (least waiting distance) + Delta when
                                       none is below it (delta-stepping).  Same distances;
                                       range [0, 2^30]; ignored on a partition handle */
+#define PM_TUNE_PULL_STAGE 14      /* pull-reduce passes (heavy mode 0, no hub cache, ids
+                                      without paired weights): 1 copies each 32-row
+                                      batch's CSC ids (up to 1024) into shared memory with
+                                      one bulk copy and reads them there; 0 (default)
+                                      reads them from global memory.  Same results */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

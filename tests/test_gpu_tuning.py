@@ -125,7 +125,7 @@ def test_tunable_range_checks(pm):
     with pm.Graph.rmat(10, 8) as g:
         for name, bad in (("heavy_deg", 10), ("cta_expand", 0), ("pull_ctas_per_sm", -1),
                           ("bfs_div", 0), ("cuda_graphs", 2), ("bf_dense", 2),
-                          ("cc_mode", -1), ("bf_delta", -1)):
+                          ("cc_mode", -1), ("bf_delta", -1), ("pull_stage", 2)):
             before = g.get_tunable(name)
             with pytest.raises(pm.PolymerError) as ei:
                 g.set_tunable(name, bad)
@@ -222,3 +222,33 @@ def test_heavy_mode_overlapped_is_bit_identical(pm):
                 got = _fp_runs(pm, g, x0, prior)
                 for a, b in zip(base, got):
                     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("scale", [10, 15])
+def test_pull_stage_bit_identical(pm, oracle, scale):
+    """Staged ids (one bulk copy of a batch's CSC ids into shared memory) read
+    the same ids in the same order: every pull-reduce result is unchanged bit
+    for bit, with batches staged, batches too long to stage and the last ids of
+    the array (read from global memory) all on the path."""
+    og = oracle.rmat_graph(scale, 16)
+    sym = oracle.rmat_graph(scale, 16, symmetric=True)
+    w = oracle.weights_int(sym)
+    srcs = oracle.pick_sources(sym, 2, seed=0x5EED0025)
+    with pm.Graph.from_csr(og.off, og.idx) as g:
+        prior = pm.uniform_f32(g, 2 * g.n, 12, open_interval=True).cpu().numpy()
+        runs = []
+        for st in (0, 1, 0, 1):
+            g.set_tunable("pull_stage", st)
+            runs.append((pm.PageRank(g, 7, dtype=np.float32), pm.PageRank(g, 4, dtype=np.float64),
+                         pm.BeliefPropagation(g, prior, 3)))
+        for r in runs[1:]:
+            for a, b in zip(runs[0], r):
+                assert np.array_equal(a, b)
+        assert rel_l1(runs[1][0], oracle.pagerank(og, 7)) < RL1_F32
+    with pm.Graph.from_csr(sym.off, sym.idx, symmetric=True) as g:
+        g.set_weights(w)
+        g.set_tunable("cc_mode", 1)  # label propagation: dense rounds pull-reduce
+        g.set_tunable("pull_stage", 1)
+        assert np.array_equal(pm.Components(g), oracle.cc(sym))
+        for s in srcs:
+            assert np.array_equal(pm.BellmanFord(g, int(s)), oracle.dijkstra(sym, w, int(s)))
