@@ -82,6 +82,7 @@ struct GraphView {
   int32_t heavy_deg = kHeavyDeg;      // rows with more edges than this are chunked
   int32_t cta_expand = kCtaExpand;    // sparse push degree bins
   int32_t grid_expand = kGridExpand;
+  int32_t push_agg = 0;               // warp-aggregated min pushes (MinPush functors)
   Adj out;  // CSR
   Adj in;   // CSC (aliases out for symmetric graphs)
 #if PM_CHECK
@@ -213,6 +214,39 @@ __device__ __forceinline__ bool push_edge(const GraphView &g, F &f, const W *w, 
   return false;
 }
 
+// A functor whose updateAtomic(s, d, w) is "atomicMin(min_target() + d,
+// push_value(s, w)) lowered the value" (Components' labels, BellmanFord's
+// distances) declares those two members; its pushes from many sources are
+// then warp-aggregated on the sparse push's short rows when the tunable
+// push_agg is set: lanes with the same target combine their values with one
+// warp reduction and the group's first lane issues a single atomicMin.  The
+// target ends at the same minimum and is activated when the minimum lowered
+// it, as with one atomic per edge.
+template <class F, class = void>
+struct MinPush : std::false_type {};
+template <class F>
+struct MinPush<F, std::void_t<decltype(std::declval<const F &>().min_target())>> : std::true_type {};
+
+// Warp-collective (every lane of the warp calls it; valid marks the lanes
+// with an edge): the aggregated form of push_edge for MinPush functors.
+template <class F, class W>
+__device__ __forceinline__ bool push_edge_min(const GraphView &g, F &f, const W *w, bool valid, int s,
+                                              int64_t e, uint32_t *next_bits, int &d_out) {
+  int d = -1;
+  int32_t v = 0x7fffffff;
+  if (valid) {
+    d = checked_id(g, __ldg(g.out.idx + e));
+    valid = f.cond(d);
+    if (valid) v = f.push_value(s, load_w(w, e));
+  }
+  d_out = d;
+  // lanes without an edge get keys no target has (ids are >= 0)
+  const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : -1 - (int)(threadIdx.x & 31));
+  const int32_t gmin = __reduce_min_sync(peers, v);
+  if (!valid || (int)(threadIdx.x & 31) != __ffs(peers) - 1) return false;
+  return gmin < atomicMin(f.min_target() + d, gmin) && set_bit_new(next_bits, d);
+}
+
 template <class F, class W>
 __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t *__restrict__ queue,
                                                      int32_t qsize, F f, const W *__restrict__ w,
@@ -304,13 +338,21 @@ __global__ void __launch_bounds__(256) k_sparse_push(GraphView g, const int32_t 
     for (int r = 0; r < total; r += 256) {
       int k = r + tid, d = -1;
       bool act = false;
+      int lo = 0;
       if (k < total) {
-        int lo = 0, hi = 255;  // last j with s_pos[j] <= k
+        int hi = 255;  // last j with s_pos[j] <= k
         while (lo < hi) {
           int mid = (lo + hi + 1) >> 1;
           if (s_pos[mid] <= k) lo = mid; else hi = mid - 1;
         }
-        act = push_edge(g, f, w, s_v[lo], (int64_t)s_o[lo] + (k - s_pos[lo]), next_bits, d);
+        if (!MinPush<F>::value || !g.push_agg)
+          act = push_edge(g, f, w, s_v[lo], (int64_t)s_o[lo] + (k - s_pos[lo]), next_bits, d);
+      }
+      // the short rows of different sources share targets (hubs): aggregate
+      if constexpr (MinPush<F>::value) {
+        if (g.push_agg)  // a kernel argument: the same branch for the whole warp
+          act = push_edge_min(g, f, w, k < total, k < total ? s_v[lo] : 0,
+                              k < total ? (int64_t)s_o[lo] + (k - s_pos[lo]) : 0, next_bits, d);
       }
       if (act) my_edges += __ldg(g.out.off + d + 1) - __ldg(g.out.off + d);
       emit_queue(act, d, next_queue, qcap, cnt);
@@ -1421,6 +1463,8 @@ struct Tunables {
                                      // bound that moves by this much (delta-stepping); 0 all
   int32_t pull_stage = 0;            // pull-reduce: 1 copies each batch's CSC ids to shared
                                      // memory with one bulk copy (unweighted / int weights)
+  int32_t push_agg = 0;              // sparse push: 1 warp-aggregates the atomicMin updates of
+                                     // Components and BellmanFord
 };
 
 // Key of a captured loop: its name and every value its launches bake in.

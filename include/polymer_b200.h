@@ -477,6 +477,10 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
                                       batch's CSC ids (up to 1024) into shared memory with
                                       one bulk copy and reads them there; 0 (default)
                                       reads them from global memory.  Same results */
+#define PM_TUNE_PUSH_AGG 15        /* sparse push rounds of Components and BellmanFord: 1
+                                      combines the atomicMin updates of a warp's lanes that
+                                      share a target (one atomic per target per warp); 0
+                                      (default) one atomic per edge.  Same results */
 /* g == NULL sets / reads the process-wide values that handles created
  * afterwards start with (so tables that depend on them are built once);
  * changing PM_TUNE_HEAVY_DEG on a handle rebuilds its heavy-row tables. */

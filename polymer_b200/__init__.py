@@ -72,7 +72,7 @@ class TuneReport(C.Structure):
 TUNABLES = {"heavy_deg": 0, "cta_expand": 1, "grid_expand": 2, "pull_ctas_per_sm": 3,
             "bfs_div": 4, "cc_div": 5, "bf_div": 6, "cuda_graphs": 7, "heavy_mode": 8,
             "hub_cache": 9, "multi_div": 10, "bf_dense": 11, "cc_mode": 12,
-            "bf_delta": 13, "pull_stage": 14}
+            "bf_delta": 13, "pull_stage": 14, "push_agg": 15}
 APPS = {"pagerank": 0, "spmv": 1, "bp": 2, "bfs": 3, "cc": 4, "bellman_ford": 5}
 
 _lib = None

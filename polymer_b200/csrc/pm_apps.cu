@@ -291,6 +291,9 @@ struct CC_F {
     int32_t v = *((volatile int32_t *)ids + s);
     return v < atomicMin(ids + d, v);
   }
+  // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
+  __device__ __forceinline__ int32_t *min_target() const { return ids; }
+  __device__ __forceinline__ int32_t push_value(int s, int) const { return *((volatile int32_t *)ids + s); }
   __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
   __device__ __forceinline__ Acc edge(int s, int, int) const {
     return test_bit(cur, s) ? *((volatile int32_t *)ids + s) : 0x7fffffff;
@@ -357,6 +360,11 @@ struct BF_F {
     int32_t nd = *((volatile int32_t *)dist + s) + w;
     return nd < atomicMin(dist + d, nd);
   }
+  // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
+  __device__ __forceinline__ int32_t *min_target() const { return dist; }
+  __device__ __forceinline__ int32_t push_value(int s, int32_t w) const {
+    return *((volatile int32_t *)dist + s) + w;
+  }
   __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
   __device__ __forceinline__ Acc edge(int s, int, int32_t w) const {
     return test_bit(cur, s) ? *((volatile int32_t *)dist + s) + w : 0x7fffffff;
@@ -384,6 +392,11 @@ struct BF_FD {
   __device__ __forceinline__ bool updateAtomic(int s, int d, int32_t w) const {
     int32_t nd = *((volatile int32_t *)dist + s) + w;
     return nd < atomicMin(dist + d, nd);
+  }
+  // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
+  __device__ __forceinline__ int32_t *min_target() const { return dist; }
+  __device__ __forceinline__ int32_t push_value(int s, int32_t w) const {
+    return *((volatile int32_t *)dist + s) + w;
   }
   __device__ __forceinline__ Acc identity() const { return 0x7fffffff; }
   __device__ __forceinline__ Acc edge(int s, int, int32_t w) const {

@@ -256,6 +256,7 @@ static void set_views(pm_graph *g) {
   v.heavy_deg = g->E.tune.heavy_deg;
   v.cta_expand = g->E.tune.cta_expand;
   v.grid_expand = g->E.tune.grid_expand;
+  v.push_agg = g->E.tune.push_agg;
 #if PM_CHECK
   if (!g->check_word.p) {
     g->check_word.alloc(16);

@@ -45,6 +45,7 @@ int32_t &field(Tunables &t, int key) {
     case PM_TUNE_CC_MODE: return t.cc_mode;
     case PM_TUNE_BF_DELTA: return t.bf_delta;
     case PM_TUNE_PULL_STAGE: return t.pull_stage;
+    case PM_TUNE_PUSH_AGG: return t.push_agg;
   }
   fail(PM_ERR_INVALID_ARG, "unknown tunable " + std::to_string(key));
 }
@@ -98,6 +99,9 @@ void check_tunable(int key, int64_t value) {
       break;
     case PM_TUNE_PULL_STAGE:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "pull_stage must be 0 or 1");
+      break;
+    case PM_TUNE_PUSH_AGG:
+      if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "push_agg must be 0 or 1");
       break;
     case PM_TUNE_BF_DELTA:
       if (value < 0 || value > (1 << 30)) fail(PM_ERR_INVALID_ARG, "bf_delta must be in [0, 2^30]");

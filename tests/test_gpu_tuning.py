@@ -125,7 +125,7 @@ def test_tunable_range_checks(pm):
     with pm.Graph.rmat(10, 8) as g:
         for name, bad in (("heavy_deg", 10), ("cta_expand", 0), ("pull_ctas_per_sm", -1),
                           ("bfs_div", 0), ("cuda_graphs", 2), ("bf_dense", 2),
-                          ("cc_mode", -1), ("bf_delta", -1), ("pull_stage", 2)):
+                          ("cc_mode", -1), ("bf_delta", -1), ("pull_stage", 2), ("push_agg", -1)):
             before = g.get_tunable(name)
             with pytest.raises(pm.PolymerError) as ei:
                 g.set_tunable(name, bad)
@@ -252,3 +252,22 @@ def test_pull_stage_bit_identical(pm, oracle, scale):
         assert np.array_equal(pm.Components(g), oracle.cc(sym))
         for s in srcs:
             assert np.array_equal(pm.BellmanFord(g, int(s)), oracle.dijkstra(sym, w, int(s)))
+
+
+@pytest.mark.parametrize("scale", [11, 15])
+def test_push_agg_results_unchanged(pm, oracle, scale):
+    """Warp-aggregated atomicMin pushes (one atomic per target per warp) give
+    the labels and distances of one atomic per edge: every round sparse, and
+    with the default direction switch."""
+    sym = oracle.rmat_graph(scale, 16, symmetric=True)
+    w = oracle.weights_int(sym)
+    srcs = oracle.pick_sources(sym, 3, seed=0x5EED0026)
+    with pm.Graph.from_csr(sym.off, sym.idx, symmetric=True) as g:
+        g.set_weights(w)
+        g.set_tunable("cc_mode", 1)
+        g.set_tunable("push_agg", 1)
+        assert g.get_tunable("push_agg") == 1
+        for thr in (1 << 40, -1):
+            assert np.array_equal(pm.Components(g, threshold=thr), oracle.cc(sym))
+            for s in srcs:
+                assert np.array_equal(pm.BellmanFord(g, int(s), threshold=thr), oracle.dijkstra(sym, w, int(s)))
