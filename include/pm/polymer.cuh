@@ -244,7 +244,8 @@ __device__ __forceinline__ bool push_edge_min(const GraphView &g, F &f, const W 
   const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : -1 - (int)(threadIdx.x & 31));
   const int32_t gmin = __reduce_min_sync(peers, v);
   if (!valid || (int)(threadIdx.x & 31) != __ffs(peers) - 1) return false;
-  return gmin < atomicMin(f.min_target() + d, gmin) && set_bit_new(next_bits, d);
+  return gmin < *((volatile int32_t *)f.min_target() + d) && gmin < atomicMin(f.min_target() + d, gmin) &&
+         set_bit_new(next_bits, d);
 }
 
 template <class F, class W>
@@ -1455,8 +1456,9 @@ struct Tunables {
                                      // 2 a launch beside it on a second stream
   int32_t hub_cache = 0;             // FP32 PageRank: sources cached in shared memory (0 = off)
   int32_t multi_div = 8;             // multi-source BFS / BellmanFord: default threshold = m / div
-  int32_t bf_dense = 0;              // BellmanFord dense rounds: 0 pull-reduce over the CSC,
-                                     // 1 push over the frontier's out-edges (DENSE_FORWARD)
+  int32_t bf_dense = 2;              // BellmanFord dense rounds: 0 pull-reduce over the CSC,
+                                     // 1 push over the frontier's out-edges (DENSE_FORWARD),
+                                     // 2 that push with atomics whose result is unused
   int32_t cc_mode = 0;               // Components on a symmetric graph: 0 union-find,
                                      // 1 label propagation (the reference's rounds)
   int32_t bf_delta = 0;              // BellmanFord: > 0 relaxes only frontier vertices below a

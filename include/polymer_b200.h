@@ -453,12 +453,17 @@ PM_API pm_status pm_profile_read(pm_graph *g, const char *tag, double *total_ms,
 #define PM_TUNE_MULTI_DIV 10       /* threshold < 0 means m / div: multi-source BFS and
                                       BellmanFord (default 8; their union frontiers turn
                                       dense sooner than one source's) */
-#define PM_TUNE_BF_DENSE 11        /* BellmanFord's dense rounds: 0 (default) a pull-reduce
+#define PM_TUNE_BF_DENSE 11        /* BellmanFord's dense rounds: 0 a pull-reduce
                                       over every in-edge (min of dist[s] + w over frontier
                                       sources); 1 a push over the frontier's out-edges with
                                       atomicMin, edgeMap's DENSE_FORWARD option, which the
-                                      reference's BellmanFord passes (numa-BellmanFord.C:182).
-                                      Ignored on a partition handle (pull only) */
+                                      reference's BellmanFord passes (numa-BellmanFord.C:182);
+                                      2 (default) the same push with atomics whose result is
+                                      unused, skipped when the target's distance is already
+                                      no larger, the next frontier taken from the distances
+                                      that fell.
+                                      Same distances; ignored on a partition handle (pull
+                                      only) */
 #define PM_TUNE_CC_MODE 12         /* Components on a symmetric whole-graph handle: 0
                                       (default) a concurrent union-find (sampled links,
                                       the largest component skipped, roots are minimum

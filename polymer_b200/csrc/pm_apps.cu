@@ -287,9 +287,10 @@ struct CC_F {
   const uint32_t *cur;
   using Acc = int32_t;
   __device__ __forceinline__ bool cond(int) const { return true; }
+  // writeMin (utils.h): nothing to do when the label is already no larger
   __device__ __forceinline__ bool updateAtomic(int s, int d, int) const {
     int32_t v = *((volatile int32_t *)ids + s);
-    return v < atomicMin(ids + d, v);
+    return v < *((volatile int32_t *)ids + d) && v < atomicMin(ids + d, v);
   }
   // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
   __device__ __forceinline__ int32_t *min_target() const { return ids; }
@@ -356,9 +357,10 @@ struct BF_F {
   const uint32_t *cur;
   using Acc = int32_t;
   __device__ __forceinline__ bool cond(int) const { return true; }
+  // writeMin (utils.h): nothing to do when the distance is already no larger
   __device__ __forceinline__ bool updateAtomic(int s, int d, int32_t w) const {
     int32_t nd = *((volatile int32_t *)dist + s) + w;
-    return nd < atomicMin(dist + d, nd);
+    return nd < *((volatile int32_t *)dist + d) && nd < atomicMin(dist + d, nd);
   }
   // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
   __device__ __forceinline__ int32_t *min_target() const { return dist; }
@@ -389,9 +391,10 @@ struct BF_FD {
   const int32_t *fd;
   using Acc = int32_t;
   __device__ __forceinline__ bool cond(int) const { return true; }
+  // writeMin (utils.h): nothing to do when the distance is already no larger
   __device__ __forceinline__ bool updateAtomic(int s, int d, int32_t w) const {
     int32_t nd = *((volatile int32_t *)dist + s) + w;
-    return nd < atomicMin(dist + d, nd);
+    return nd < *((volatile int32_t *)dist + d) && nd < atomicMin(dist + d, nd);
   }
   // updateAtomic as an atomicMin of push_value (warp-aggregated pushes)
   __device__ __forceinline__ int32_t *min_target() const { return dist; }
@@ -420,6 +423,146 @@ __global__ void k_bf_snapshot(int32_t n, const uint32_t *__restrict__ bits, cons
     fd[v] = test_bit(bits, (int)v) ? dist[v] : 0x7fffffff;
 }
 
+// Dense BellmanFord round as a push whose atomics return nothing
+// (PM_TUNE_BF_DENSE 2).  The frontier's rows (light ones here, heavy ones by
+// 4096-edge chunks below) relax their out-edges with atomicMin whose result
+// is unused, so the warp never waits for an atomic; each lane takes
+// kBfRedEdges consecutive edges of a window and issues their id and weight
+// loads before their atomics, and skips the atomic when the target's
+// distance, as this SM last saw it, is already no larger (distances only
+// fall, so a value seen earlier is never below the current one; the hub
+// targets would otherwise take an atomic from most of their in-edges every
+// round, one after another at one L2 slice).  A source's distance is read once, at its
+// batch's start: a source lowered later in the round is in the next frontier
+// and pushes again, so the rounds end at the same distances.  The next
+// frontier is what fell during the round: k_bf_fell compares the distances
+// with a copy taken before it.
+constexpr int kBfRedEdges = 4;
+
+__global__ void __launch_bounds__(256) k_bf_push_red(GraphView g, const uint32_t *__restrict__ cur,
+                                                     const int32_t *__restrict__ w, int32_t *dist) {
+  __shared__ int s_pos[8][33];
+  __shared__ int s_off[8][32];
+  __shared__ int32_t s_ds[8][32];
+  const int lane = lane_id(), wid = threadIdx.x >> 5;
+  const int grp = blockIdx.x * 8 + wid;
+  if (grp >= g.out.ngroups) return;
+  int *pos_s = s_pos[wid], *off_s = s_off[wid];
+  int32_t *ds_s = s_ds[wid];
+  const int r_begin = __ldg(g.out.gstart + grp), r_end = __ldg(g.out.gstart + grp + 1);
+  for (int rb = r_begin; rb < r_end; rb += 32) {  // group starts are multiples of 32
+    const uint32_t word = __ldg(cur + (rb >> 5));
+    if (word == 0) continue;
+    const int r = rb + lane;
+    int o0 = 0, deg = 0;
+    int32_t ds = 0;
+    if (r < r_end && ((word >> lane) & 1u)) {
+      o0 = __ldg(g.out.off + r);
+      deg = __ldg(g.out.off + r + 1) - o0;
+      ds = *((volatile const int32_t *)dist + r);
+      if (deg > g.heavy_deg || ds >= kDevBFInf) deg = 0;
+    }
+    int total;
+    const int pos = warp_excl_scan(deg, &total);
+    __syncwarp();  // the previous batch's windows are done with the arrays
+    pos_s[lane] = pos;
+    if (lane == 31) pos_s[32] = total;
+    off_s[lane] = o0;
+    ds_s[lane] = ds;
+    __syncwarp();
+    for (int c = 0; c < total; c += 32 * kBfRedEdges) {
+      const int q0 = c + lane * kBfRedEdges;
+      if (q0 >= total) continue;
+      int j = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1)
+        if (pos_s[j + step] <= q0) j += step;
+      int nxt = pos_s[j + 1];
+      int32_t dst[kBfRedEdges], nd[kBfRedEdges];
+#pragma unroll
+      for (int k = 0; k < kBfRedEdges; ++k) {
+        const int q = q0 + k;
+        dst[k] = -1;
+        if (q < total) {
+          while (q >= nxt) nxt = pos_s[++j + 1];
+          const int64_t e = (int64_t)off_s[j] + (q - pos_s[j]);
+          dst[k] = checked_id(g, __ldg(g.out.idx + e));
+          nd[k] = ds_s[j] + __ldg(w + e);
+        }
+      }
+      int32_t seen[kBfRedEdges];
+#pragma unroll
+      for (int k = 0; k < kBfRedEdges; ++k) seen[k] = dst[k] >= 0 ? __ldca(dist + dst[k]) : 0;
+#pragma unroll
+      for (int k = 0; k < kBfRedEdges; ++k)
+        if (dst[k] >= 0 && nd[k] < seen[k]) atomicMin(dist + dst[k], nd[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_bf_heavy_red(GraphView g, const uint32_t *__restrict__ cur,
+                                                                const int32_t *__restrict__ w, int32_t *dist) {
+  const int c = blockIdx.x;
+  if (c >= g.out.nchunks) return;
+  const int r = __ldg(g.out.hrow + c);
+  if (!test_bit(cur, r)) return;
+  const int32_t ds = *((volatile const int32_t *)dist + r);
+  if (ds >= kDevBFInf) return;
+  const int k = c - __ldg(g.out.hfirst + r);
+  const int64_t e0 = (int64_t)__ldg(g.out.off + r) + (int64_t)k * kChunkEdges;
+  const int64_t e1 = min(e0 + kChunkEdges, (int64_t)__ldg(g.out.off + r + 1));
+  for (int64_t e = e0 + threadIdx.x; e < e1; e += kChunkThreads) {
+    const int d = checked_id(g, __ldg(g.out.idx + e));
+    const int32_t nd = ds + __ldg(w + e);
+    if (nd < __ldca(dist + d)) atomicMin(dist + d, nd);
+  }
+}
+
+// next = {v : dist[v] < before[v]}, with its size and out-degree sum.
+__global__ void k_bf_fell(int32_t n, const int32_t *__restrict__ out_off, const int32_t *__restrict__ dist,
+                          const int32_t *__restrict__ before, uint32_t *__restrict__ next, Counters *c) {
+  const int64_t ntot = ((int64_t)n + 31) & ~31ll;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long s = 0, e = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += stride) {
+    const int v = (int)t;
+    const bool fell = v < n && __ldcs(dist + v) < __ldcs(before + v);
+    const unsigned word = __ballot_sync(0xffffffffu, fell);
+    if (lane_id() == 0) next[v >> 5] = word;
+    if (fell) {
+      s++;
+      e += __ldg(out_off + v + 1) - __ldg(out_off + v);
+    }
+  }
+  s = warp_sum(s);
+  e = warp_sum(e);
+  if (lane_id() == 0 && s) {
+    atomicAdd(&c->size, s);
+    atomicAdd(&c->edges, e);
+  }
+}
+
+static void bf_round_red(pm_graph *g, VertexSubset &from, VertexSubset &next, int32_t *d_dist,
+                         const int32_t *w_out) {
+  Engine &E = g->E;
+  const int64_t n = g->n;
+  int32_t *before = (int32_t *)g->scratch_buf(37, (size_t)n * 4);
+  Counters *dc = (Counters *)g->scratch_buf(32, 2 * sizeof(Counters));
+  PM_CUDA(cudaMemcpyAsync(before, d_dist, (size_t)n * 4, cudaMemcpyDeviceToDevice, E.stream));
+  if (E.g.out.nchunks > 0)
+    PM_LAUNCH(k_bf_heavy_red, E.g.out.nchunks, kChunkThreads, 0, E.stream, E.g, from.bits, w_out, d_dist);
+  PM_LAUNCH(k_bf_push_red, (E.g.out.ngroups + 7) / 8, 256, 0, E.stream, E.g, from.bits, w_out, d_dist);
+  PM_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), E.stream));
+  PM_LAUNCH(k_bf_fell, E.grid_for(n, 256, 16), 256, 0, E.stream, (int32_t)n, E.g.out.off, d_dist, before,
+            next.bits, dc);
+  Counters hc;
+  PM_CUDA(cudaMemcpyAsync(&hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, E.stream));
+  PM_CUDA(cudaStreamSynchronize(E.stream));
+  next.size = (int64_t)hc.size;
+  next.edges = (int64_t)hc.edges;
+  next.has_queue = false;
+}
+
 // One BellmanFord round from `from` into `next`: the reference's dense push
 // (DENSE_FORWARD) when push, else the pull-reduce, which for a dense round
 // reads the frontier's distances from a snapshot.
@@ -428,6 +571,9 @@ static void bf_round(pm_graph *g, VertexSubset &from, VertexSubset &next, int64_
   Engine &E = g->E;
   if (push) {
     edgeMap<int32_t>(E, from, BF_F{d_dist, from.bits}, next, threshold, DENSE_FORWARD, w_out, w_in, dense);
+  } else if (E.tune.bf_dense == 2 && go_dense(from, threshold) && !g->is_part) {
+    bf_round_red(g, from, next, d_dist, w_out);
+    *dense = true;
   } else if (go_dense(from, threshold) && !g->is_part) {
     int32_t *fd = (int32_t *)g->scratch_buf(36, (size_t)g->n * 4);
     PM_LAUNCH(k_bf_snapshot, E.grid_for(g->n, 256, 16), 256, 0, E.stream, (int32_t)g->n, from.bits, d_dist, fd);

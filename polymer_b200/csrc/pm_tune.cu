@@ -92,7 +92,7 @@ void check_tunable(int key, int64_t value) {
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cuda_graphs must be 0 or 1");
       break;
     case PM_TUNE_BF_DENSE:
-      if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "bf_dense must be 0 or 1");
+      if (value < 0 || value > 2) fail(PM_ERR_INVALID_ARG, "bf_dense must be 0, 1 or 2");
       break;
     case PM_TUNE_CC_MODE:
       if (value != 0 && value != 1) fail(PM_ERR_INVALID_ARG, "cc_mode must be 0 or 1");
@@ -260,7 +260,7 @@ void tune(pm_graph *g, const int *apps, int count, pm_tune_report *rep) {
         case PM_TUNE_CTA_EXPAND: cands = {64, 128, 256, 512}; break;
         case PM_TUNE_GRID_EXPAND: cands = {128, 256, 512, 1024, 4096}; break;
         case PM_TUNE_HEAVY_MODE: cands = {0, 1, 2}; break;
-        case PM_TUNE_BF_DENSE: cands = {0, 1}; break;
+        case PM_TUNE_BF_DENSE: cands = {0, 1, 2}; break;
         case PM_TUNE_BF_DELTA: cands = {0, 4, 8, 16, 32}; break;
         case PM_TUNE_PULL_CTAS_PER_SM:
           cands.push_back(0);

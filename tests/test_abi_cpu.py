@@ -72,7 +72,7 @@ def test_default_tunables_host_only():
     range-checked and restored without a GPU."""
     import polymer_b200 as pm
     defaults = {"heavy_deg": 1024, "cta_expand": 128, "grid_expand": 256, "pull_ctas_per_sm": 0,
-                "bfs_div": 20, "cc_div": 8, "bf_div": 20, "cuda_graphs": 1, "multi_div": 8, "bf_dense": 0,
+                "bfs_div": 20, "cc_div": 8, "bf_div": 20, "cuda_graphs": 1, "multi_div": 8, "bf_dense": 2,
                 "cc_mode": 0, "bf_delta": 0, "pull_stage": 0, "push_agg": 0}
     assert {k: pm.get_default_tunable(k) for k in defaults} == defaults
     try:

@@ -93,7 +93,7 @@ def test_components_scale22(pm, oracle, graph_a, pool):
     assert np.array_equal(pm.Components(g), ref.result())
 
 
-@pytest.mark.parametrize("bf_dense", [0, 1])
+@pytest.mark.parametrize("bf_dense", [0, 1, 2])
 def test_bellman_ford_scale22(pm, oracle, graph_a, pool, bf_dense):
     g, og, w, srcs = graph_a
     ref = pool.submit(oracle.dijkstra, og, w, srcs[0])

@@ -293,20 +293,24 @@ def test_bellman_ford_exact(pm, oracle, threshold):
                 assert np.array_equal(d, oracle.dijkstra(og, w, int(s)))
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("threshold", [-1, 0])
-def test_bellman_ford_dense_push_exact(pm, oracle, threshold):
-    """Dense rounds through edgeMap's DENSE_FORWARD push (k_dense_push over
-    the frontier's out-edges, k_heavy_push for rows above the heavy cut-off),
-    the option the reference's BellmanFord passes (numa-BellmanFord.C:182):
-    distances equal Dijkstra's on R-MAT graphs of both kinds, with the heavy
-    cut-off at its default and lowered so that the chunk kernel runs."""
+def test_bellman_ford_dense_push_exact(pm, oracle, threshold, mode):
+    """Dense rounds pushed over the frontier's out-edges: mode 1 through
+    edgeMap's DENSE_FORWARD push (k_dense_push, k_heavy_push for rows above
+    the heavy cut-off), the option the reference's BellmanFord passes
+    (numa-BellmanFord.C:182); mode 2 with atomics whose result is unused and
+    the next frontier from the distances that fell (k_bf_push_red,
+    k_bf_heavy_red, k_bf_fell).  Distances equal Dijkstra's on R-MAT graphs
+    of both kinds, with the heavy cut-off at its default and lowered so that
+    the chunk kernels run."""
     for sym, scale in ((True, 13), (False, 13)):
         og = oracle.rmat_graph(scale, 16, symmetric=sym)
         w = oracle.weights_int(og)
         for heavy in (1024, 64):
             with dev_graph(pm, og, symmetric=sym) as g:
                 g.set_weights(w)
-                g.set_tunable("bf_dense", 1)
+                g.set_tunable("bf_dense", mode)
                 g.set_tunable("heavy_deg", heavy)
                 for s in oracle.pick_sources(og, 3):
                     d, st = pm.BellmanFord(g, int(s), threshold=threshold, stats=True)
@@ -315,7 +319,7 @@ def test_bellman_ford_dense_push_exact(pm, oracle, threshold):
                         assert st["dense_rounds"] == st["rounds"]
 
 
-@pytest.mark.parametrize("bf_dense", [0, 1])
+@pytest.mark.parametrize("bf_dense", [0, 1, 2])
 @pytest.mark.parametrize("delta", [1, 4, 16, 1 << 20])
 def test_bellman_ford_delta_stepping_exact(pm, oracle, delta, bf_dense):
     """The delta-stepping schedule (bf_delta): only frontier vertices below a
@@ -339,7 +343,8 @@ def test_bellman_ford_delta_stepping_exact(pm, oracle, delta, bf_dense):
                     assert np.array_equal(pm.BellmanFord(g, s, threshold=thr), want), (delta, thr, s)
 
 
-def test_bellman_ford_dense_push_hub(pm, oracle):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_bellman_ford_dense_push_hub(pm, oracle, mode):
     """A hub of in- and out-degree 12287 on a ring (three heavy chunks per
     direction, a ragged last chunk): every round dense, pushed."""
     n = 12288
@@ -349,7 +354,7 @@ def test_bellman_ford_dense_push_hub(pm, oracle):
     w = oracle.weights_int(og)
     with dev_graph(pm, og) as g:
         g.set_weights(w)
-        g.set_tunable("bf_dense", 1)
+        g.set_tunable("bf_dense", mode)
         for s in (5, 0, 7000, 12287):
             assert np.array_equal(pm.BellmanFord(g, s, threshold=0), oracle.dijkstra(og, w, s))
 

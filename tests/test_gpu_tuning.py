@@ -124,7 +124,7 @@ def test_direction_divisors(pm, oracle, div):
 def test_tunable_range_checks(pm):
     with pm.Graph.rmat(10, 8) as g:
         for name, bad in (("heavy_deg", 10), ("cta_expand", 0), ("pull_ctas_per_sm", -1),
-                          ("bfs_div", 0), ("cuda_graphs", 2), ("bf_dense", 2),
+                          ("bfs_div", 0), ("cuda_graphs", 2), ("bf_dense", 3),
                           ("cc_mode", -1), ("bf_delta", -1), ("pull_stage", 2), ("push_agg", -1)):
             before = g.get_tunable(name)
             with pytest.raises(pm.PolymerError) as ei:
