@@ -302,12 +302,14 @@ __global__ void __launch_bounds__(256) k_bf_multi_push(const int32_t *__restrict
         olo[u] = nlo[u] < kDevBFInf ? *(volatile int32_t *)(dist + (int64_t)dj[u] * kLanes + lane) : 0;
         ohi[u] = nhi[u] < kDevBFInf ? *(volatile int32_t *)(dist + (int64_t)dj[u] * kLanes + 32 + lane) : 0;
       }
+      // A lane below the distance read above lowers it with an atomic
+      // whose result is unused and is marked active: it fell, or another
+      // push lowered it further meanwhile (an extra relaxation next round,
+      // the same distances).
 #pragma unroll
       for (int u = 0; u < kBfPushUnroll; ++u) {
-        if (nlo[u] < olo[u]) olo[u] = atomicMin(dist + (int64_t)dj[u] * kLanes + lane, nlo[u]);
-        else nlo[u] = kDevBFInf;
-        if (nhi[u] < ohi[u]) ohi[u] = atomicMin(dist + (int64_t)dj[u] * kLanes + 32 + lane, nhi[u]);
-        else nhi[u] = kDevBFInf;
+        if (nlo[u] < olo[u]) atomicMin(dist + (int64_t)dj[u] * kLanes + lane, nlo[u]);
+        if (nhi[u] < ohi[u]) atomicMin(dist + (int64_t)dj[u] * kLanes + 32 + lane, nhi[u]);
       }
 #pragma unroll
       for (int u = 0; u < kBfPushUnroll; ++u) {
