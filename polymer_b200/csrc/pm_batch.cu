@@ -433,30 +433,48 @@ __global__ void k_bf_multi_seed(const int32_t *sources, int k, int32_t *dist, u6
   }
 }
 
-// dist vertex-major (n x 64) -> out source-major (k x n), through 32x32
-// tiles; c->size counts the finite distances (reached (source, vertex) pairs).
-__global__ void k_bf_multi_transpose(const int32_t *__restrict__ dist, int64_t n, int k,
-                                     int32_t *__restrict__ out, Counters *c) {
-  __shared__ int32_t tile[32][33];
-  const int64_t v0 = (int64_t)blockIdx.x * 32;
-  const int l0 = blockIdx.y * 32;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int64_t v = v0 + r;
-    tile[r][threadIdx.x] = v < n ? dist[v * kLanes + l0 + threadIdx.x] : kDevBFInf;
-  }
+// One count per block: the warps' sums meet in shared memory and thread 0
+// adds the block's total (blockDim = 32 x 8), so a transpose of millions of
+// tiles issues one atomic per block instead of one per warp.
+__device__ __forceinline__ void block_count_add(unsigned long long v, unsigned long long *dst) {
+  __shared__ unsigned long long s_part[8];
+  v = warp_sum(v);
+  const int w = threadIdx.y;  // one warp per threadIdx.y (blockDim.x == 32)
+  if (threadIdx.x == 0) s_part[w] = v;
   __syncthreads();
-  unsigned long long reached = 0;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int l = l0 + r;
-    const int64_t v = v0 + threadIdx.x;
-    if (l < k && v < n) {
-      const int32_t x = tile[threadIdx.x][r];
-      out[(int64_t)l * n + v] = x;
-      reached += x < kDevBFInf;
-    }
+  if (threadIdx.x == 0 && w == 0) {
+    unsigned long long t = 0;
+    for (int i = 0; i < (int)blockDim.y; ++i) t += s_part[i];
+    if (t) atomicAdd(dst, t);
   }
-  reached = warp_sum(reached);
-  if (lane_id() == 0 && reached) atomicAdd(&c->size, reached);
+}
+
+// dist vertex-major (n x 64) -> out source-major (k x n), through 32x32
+// tiles (grid-stride over the vertex tiles); c->size counts the finite
+// distances (reached (source, vertex) pairs).
+__global__ void __launch_bounds__(256) k_bf_multi_transpose(const int32_t *__restrict__ dist, int64_t n, int k,
+                                                            int32_t *__restrict__ out, Counters *c) {
+  __shared__ int32_t tile[32][33];
+  const int l0 = blockIdx.y * 32;
+  unsigned long long reached = 0;
+  for (int64_t v0 = (int64_t)blockIdx.x * 32; v0 < n; v0 += (int64_t)gridDim.x * 32) {
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t v = v0 + r;
+      tile[r][threadIdx.x] = v < n ? dist[v * kLanes + l0 + threadIdx.x] : kDevBFInf;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int l = l0 + r;
+      const int64_t v = v0 + threadIdx.x;
+      if (l < k && v < n) {
+        const int32_t x = tile[threadIdx.x][r];
+        out[(int64_t)l * n + v] = x;
+        reached += x < kDevBFInf;
+      }
+    }
+    __syncthreads();
+  }
+  block_count_add(reached, &c->size);
 }
 
 void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_out, int64_t threshold,
@@ -520,7 +538,7 @@ void run_bf_multi(pm_graph *g, const int32_t *d_sources, int k, int32_t *d_dist_
     std::swap(act, nxt);
   }
   PM_CUDA(cudaMemsetAsync(E.d_cnt + 2, 0, sizeof(Counters), E.stream));
-  dim3 tb(32, 8), tg((unsigned)((n + 31) / 32), 2);
+  dim3 tb(32, 8), tg((unsigned)std::min<int64_t>((n + 31) / 32, (int64_t)E.num_sms * 16), 2);
   PM_LAUNCH(k_bf_multi_transpose, tg, tb, 0, E.stream, dist, n, k, d_dist_out, E.d_cnt + 2);
   s.reached = (int64_t)E.read_counters()[2].size;
   if (st) *st = s;

@@ -359,10 +359,12 @@ def test_bellman_ford_dense_push_hub(pm, oracle, mode):
             assert np.array_equal(pm.BellmanFord(g, s, threshold=0), oracle.dijkstra(og, w, s))
 
 
-def _bf_multi_check(pm, oracle, og, sym, srcs, threshold):
+def _bf_multi_check(pm, oracle, og, sym, srcs, threshold, heavy_deg=None):
     w = oracle.weights_int(og)
     with dev_graph(pm, og, symmetric=sym) as g:
         g.set_weights(w)
+        if heavy_deg is not None:
+            g.set_tunable("heavy_deg", heavy_deg)
         dist, st = pm.BellmanFordMulti(srcs, g, threshold=threshold, stats=True)
     reached = 0
     for l, s in enumerate(srcs):
@@ -381,6 +383,15 @@ def test_bellman_ford_multi_matches_dijkstra(pm, oracle, threshold, sym, k):
     if k == 64:
         srcs[9] = srcs[2]  # a repeated source must give identical rows
     _bf_multi_check(pm, oracle, og, sym, srcs, threshold)
+
+
+@pytest.mark.parametrize("threshold", [-1, 0])
+def test_bellman_ford_multi_heavy_pieces(pm, oracle, threshold):
+    # heavy rows from in-degree 64: most dense-round work goes through the
+    # 512-edge pieces and their atomicMin updates
+    og = oracle.rmat_graph(14, 16, symmetric=True)
+    srcs = oracle.pick_sources(og, 64, seed=0x5EED0017)
+    _bf_multi_check(pm, oracle, og, True, srcs, threshold, heavy_deg=64)
 
 
 @pytest.mark.parametrize("threshold", [-1, 0, 1 << 40])
