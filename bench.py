@@ -293,11 +293,12 @@ def e2e_run(pm, suite, steps, pipeline_steps):
 
     Two schedules of the same steps.  `serial`: one host thread, each graph
     built, run and destroyed before the next is built.  The headline
-    (`value`): the two graphs of a step are independent workloads, each with
-    a builder thread that uploads and builds its next graph (own stream, the
-    copy engines) while a runner thread runs the applications on its current
-    one (own stream, the SMs) -- graph handles are independent, and the
-    library's calls release the interpreter lock.  Every step's uploads and
+    (`value`): one builder thread uploads and builds the graphs in step order
+    (A, B, A, B, ...; the uploads share one host link, so one builder keeps it
+    busy) up to two graphs ahead of each runner, while one runner thread per
+    graph kind runs the applications on its current graph (own stream, the
+    SMs) -- graph handles are independent, and the library's calls release
+    the interpreter lock.  Every step's uploads and
     result reads are inside the timed region; the time is the host clock
     from the first upload to the last result, over the steps."""
     import queue
@@ -379,8 +380,8 @@ def e2e_run(pm, suite, steps, pipeline_steps):
               "phases_s": {k: round(v, 4) for k, v in zip(names, phases[i])},
               "timing": "host clock around synchronous API calls, median of %d steps after an untimed one" % steps}
 
-    # pipelined schedule: per graph kind, a builder at most two graphs ahead
-    # of its runner
+    # pipelined schedule: one builder, at most two graphs of each kind ahead
+    # of that kind's runner
     failure, total = [], {"A": 0, "B": 0}
     queues = {"A": queue.Queue(maxsize=1), "B": queue.Queue(maxsize=1)}
     n_steps = [pipeline_steps]
@@ -403,12 +404,13 @@ def e2e_run(pm, suite, steps, pipeline_steps):
                 if failure:
                     return None
 
-    def builder(which):
+    def builder():
         try:
             for _ in range(n_steps[0]):
-                if not put(queues[which], build(which)):
-                    return
-        except BaseException as exc:  # the runner stops on its next wait
+                for which in ("A", "B"):
+                    if not put(queues[which], build(which)):
+                        return
+        except BaseException as exc:  # the runners stop on their next wait
             failure.append(exc)
 
     def runner(which):
@@ -427,7 +429,8 @@ def e2e_run(pm, suite, steps, pipeline_steps):
         total["A"] = total["B"] = 0
         suite.torch.cuda.synchronize()
         t0 = time.perf_counter()
-        threads = [threading.Thread(target=f, args=(w,), daemon=True) for w in ("A", "B") for f in (builder, runner)]
+        threads = [threading.Thread(target=builder, daemon=True)] + \
+            [threading.Thread(target=runner, args=(w,), daemon=True) for w in ("A", "B")]
         for th in threads:
             th.start()
         for th in threads:
@@ -451,8 +454,8 @@ def e2e_run(pm, suite, steps, pipeline_steps):
             "d2h_bytes_per_step": int(d2h), "seconds_per_step": round(t / pipeline_steps, 4),
             "edges_per_step": int(edges // pipeline_steps), "cached_bytes_after": pm.memory_cached(),
             "timing": "host clock from the first upload to the last result read, %d steps after 3 untimed "
-                      "ones; per graph kind a builder thread uploads and builds the next graph while a "
-                      "runner thread runs the current one" % pipeline_steps,
+                      "ones; one builder thread uploads and builds the graphs in step order while one "
+                      "runner thread per graph kind runs the current one" % pipeline_steps,
             "serial": serial}
 
 
