@@ -286,7 +286,7 @@ def use_tunables(pm, like):
         pm.set_default_tunable(k, v)
 
 
-def e2e_run(pm, suite, steps, pipeline_steps):
+def e2e_run(pm, suite, steps, pipeline_steps, device=0):
     """Suite through the public API from pinned host CSR arrays, per step:
     upload + build both graphs, set weights, run, read every result back
     into preallocated pinned host buffers.
@@ -445,7 +445,10 @@ def e2e_run(pm, suite, steps, pipeline_steps):
     # untimed: the pipeline keeps more graphs alive than the serial schedule;
     # their first builds would take their blocks from cudaMalloc
     pipelined(3)
+    clocks = ClockSampler(device)
+    clocks.start()
     t = pipelined(pipeline_steps)
+    clk = clocks.stop()
     for a in list(hA.values()) + list(hB.values()) + oA["par"] + oA["dep"] + [oA["lab"], oA["dist"]] + \
             list(oB.values()):
         a.free()
@@ -456,7 +459,7 @@ def e2e_run(pm, suite, steps, pipeline_steps):
             "timing": "host clock from the first upload to the last result read, %d steps after 3 untimed "
                       "ones; one builder thread uploads and builds the graphs in step order while one "
                       "runner thread per graph kind runs the current one" % pipeline_steps,
-            "serial": serial}
+            "clocks": clk, "serial": serial}
 
 
 def batched_block(pm, suite, reps=3):
@@ -917,7 +920,7 @@ def main():
     # batched, adjoint and ingest workloads) leave host and device state that
     # a process serving this suite would not have
     if not args.no_e2e:
-        e2e = e2e_run(pm, suite, args.e2e_steps, args.e2e_pipeline_steps)
+        e2e = e2e_run(pm, suite, args.e2e_steps, args.e2e_pipeline_steps, local)
         if dist:  # whole job: every rank's edges over the slowest rank's step
             ms_max, edges_all = aggregate_ranks(dist, 1e3 * e2e["seconds_per_step"], e2e["edges_per_step"], "cuda")
             e2e.update(value=round(edges_all / (ms_max / 1e3) / 1e9, 4), seconds_per_step=round(ms_max / 1e3, 4),
