@@ -381,8 +381,16 @@ def e2e_run(pm, suite, steps, pipeline_steps, device=0):
               "timing": "host clock around synchronous API calls, median of %d steps after an untimed one" % steps}
 
     # pipelined schedule: one builder, at most two graphs of each kind ahead
-    # of that kind's runner
+    # of that kind's runner; every build and run is timed (host clock) so the
+    # line can show where a slow step went
     failure, total = [], {"A": 0, "B": 0}
+    spans = []  # (kind, "build" | "run", seconds)
+
+    def timed(kind, phase, fn, *a):
+        t_0 = time.perf_counter()
+        r = fn(*a)
+        spans.append((kind, phase, time.perf_counter() - t_0))
+        return r
     queues = {"A": queue.Queue(maxsize=1), "B": queue.Queue(maxsize=1)}
     n_steps = [pipeline_steps]
 
@@ -408,7 +416,7 @@ def e2e_run(pm, suite, steps, pipeline_steps, device=0):
         try:
             for _ in range(n_steps[0]):
                 for which in ("A", "B"):
-                    if not put(queues[which], build(which)):
+                    if not put(queues[which], timed(which, "build", build, which)):
                         return
         except BaseException as exc:  # the runners stop on their next wait
             failure.append(exc)
@@ -420,7 +428,7 @@ def e2e_run(pm, suite, steps, pipeline_steps, device=0):
                 if g is None:
                     return
                 with g:
-                    total[which] += run(which, g)
+                    total[which] += timed(which, "run", run, which, g)
         except BaseException as exc:
             failure.append(exc)
 
@@ -447,8 +455,16 @@ def e2e_run(pm, suite, steps, pipeline_steps, device=0):
     pipelined(3)
     clocks = ClockSampler(device)
     clocks.start()
+    del spans[:]
     t = pipelined(pipeline_steps)
     clk = clocks.stop()
+    phases_p = {}
+    for kind in ("A", "B"):
+        for phase in ("build", "run"):
+            d = [x[2] for x in spans if x[0] == kind and x[1] == phase]
+            if d:
+                phases_p["%s_%s" % (phase, kind)] = {"mean_s": round(float(np.mean(d)), 4),
+                                                     "max_s": round(float(np.max(d)), 4)}
     for a in list(hA.values()) + list(hB.values()) + oA["par"] + oA["dep"] + [oA["lab"], oA["dist"]] + \
             list(oB.values()):
         a.free()
@@ -459,7 +475,7 @@ def e2e_run(pm, suite, steps, pipeline_steps, device=0):
             "timing": "host clock from the first upload to the last result read, %d steps after 3 untimed "
                       "ones; one builder thread uploads and builds the graphs in step order while one "
                       "runner thread per graph kind runs the current one" % pipeline_steps,
-            "clocks": clk, "serial": serial}
+            "clocks": clk, "phases": phases_p, "serial": serial}
 
 
 def batched_block(pm, suite, reps=3):
